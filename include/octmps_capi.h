@@ -1,0 +1,238 @@
+/*
+ * octmps_capi.h - C ABI of the B200 OCT-MPS photon-transport library.
+ *
+ * The reference (SSSherif/OCT-MPS) has no library interface: its host
+ * program calls a per-GPU worker, RunGPUi(HostThreadState*)
+ * (src/main.cu:43), which allocates every device buffer, uploads the mesh,
+ * runs the kernels and copies the tallies back, once per A-scan.  This
+ * header is the boundary that replaces it.  Plain C types and pointers only;
+ * every call returns an octmps_status and never exits the process.
+ *
+ * Units are the reference's: lengths in cm, coefficients in 1/cm.
+ *
+ * Entry point                      replaces (reference file:line)
+ * -------------------------------  -----------------------------------------
+ * octmps_ctx_create/destroy        device setup / cudaDeviceReset in main
+ *                                  (src/main.cu:877-888, 1054)
+ * octmps_mesh_build_file           MeshGraph + FindRootofGraph +
+ * octmps_mesh_find_root            SerializeGraph (src/mesh.cpp:86-359)
+ * octmps_mesh_upload/release       mesh upload inside RunGPUi
+ *                                  (src/main.cu:447-465), made resident
+ * octmps_rng_init                  init_RNG (src/octmps_kernel.cuh:52-172)
+ * octmps_job_submit/wait/fetch     RunGPUi (src/main.cu:43-660) with
+ *                                  InitDeviceConstantMemory
+ *                                  (src/octmps_kernel.cuh:177-220) and
+ *                                  CopyDeviceToHostMem (:225-300)
+ * octmps_read_opt / octmps_read_mci read_simulation_data
+ *                                  (src/octmps_io.cpp:504-645), Bias_Read
+ *                                  (src/bias.cpp:9-110)
+ * octmps_write_result              Write_Bias_Parameters + WriteResult
+ *                                  (src/octmps_io.cpp:237-437)
+ */
+#ifndef OCTMPS_CAPI_H
+#define OCTMPS_CAPI_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    OCTMPS_OK = 0,
+    OCTMPS_ERR_INVALID_ARG = 1, /* bad pointer, size or parameter */
+    OCTMPS_ERR_OOM = 2,         /* device or host allocation failed */
+    OCTMPS_ERR_DEVICE = 3,      /* CUDA error; the message says which */
+    OCTMPS_ERR_TIMEOUT = 4,     /* octmps_job_wait ran out of time */
+    OCTMPS_ERR_NOT_FOUND = 5,   /* unknown mesh or job id */
+    OCTMPS_ERR_IO = 6,          /* file could not be read or written */
+    OCTMPS_ERR_NO_DEVICE = 7,   /* no CUDA device, or not sm_100 */
+    OCTMPS_ERR_BUDGET = 8,      /* admission refused: HBM budget exceeded */
+    OCTMPS_ERR_KERNEL = 9       /* a kernel reported an internal error word */
+} octmps_status;
+
+/* Arithmetic of one job.  MIXED: geometry, direction, weight and scattering
+ * in FP32, optical path length, depth bin and tally sums in FP64 (the
+ * default).  FP32: everything in FP32.  FP64: everything in FP64, the
+ * precision of the reference. */
+typedef enum { OCTMPS_PREC_MIXED = 0, OCTMPS_PREC_FP32 = 1, OCTMPS_PREC_FP64 = 2 } octmps_precision;
+
+typedef struct octmps_ctx octmps_ctx;
+typedef int32_t octmps_mesh_id;
+typedef int64_t octmps_job_id;
+
+/* ---- mesh ---------------------------------------------------------------
+ * A tetrahedral mesh in the layout SerializeGraph produces
+ * (TetrahedronStructGPU and TriangleFaces, src/octmps.h:52-57,193-196):
+ * per tet its 1-based region, 4 face indices, 4 orientation signs (+1/-1)
+ * and 4 neighbour tets (-1 = boundary, the ambient medium); per face the
+ * plane Nx*x + Ny*y + Nz*z + d = 0.  Sign s on face f orients the plane so
+ * that (N*s).x + d*s > 0 inside the tet. */
+typedef struct {
+    int32_t n_tets;
+    int32_t n_faces;
+    const int32_t *tet_region; /* [n_tets] */
+    const int32_t *tet_faces;  /* [n_tets*4] */
+    const int32_t *tet_signs;  /* [n_tets*4] */
+    const int32_t *tet_adj;    /* [n_tets*4] */
+    const double *face_plane;  /* [n_faces*4]: Nx, Ny, Nz, d */
+} octmps_mesh_desc;
+
+/* Host-side mesh built from a .mesh file; arrays owned by the library,
+ * freed by octmps_mesh_host_free. */
+typedef struct {
+    int32_t n_vertices;
+    int32_t n_tets;
+    int32_t n_faces;     /* 4*n_tets slots, as the reference sizes them */
+    int32_t n_distinct;  /* faces actually used */
+    int32_t *tet_region;
+    int32_t *tet_faces;
+    int32_t *tet_signs;
+    int32_t *tet_adj;
+    double *face_plane;
+} octmps_host_mesh;
+
+/* ---- simulation parameters (SimulationStruct, src/octmps.h:77-128) ---- */
+typedef struct {
+    double n, mua, mus, g; /* as read from the .opt file */
+} octmps_region;
+
+#define OCTMPS_MAX_REGIONS 100 /* including the ambient region 0 */
+
+typedef struct {
+    double start_x, step_x, end_x; /* probe scan, x only (y = z = 0) */
+    uint32_t number_of_photons;
+    int32_t n_regions;                          /* including ambient region 0 */
+    octmps_region regions[OCTMPS_MAX_REGIONS];  /* [0].n = ambient index */
+    int32_t type_simulation;
+    int32_t type_bias; /* 0: HG only; 37: biased toward the probe; 3: no split */
+    int32_t record_photons_flag;
+    int32_t num_optical_depth_length_steps; /* depth bins, NBINS */
+    double backward_bias_coefficient;
+    double target_depth_min, target_depth_max;
+    double coherence_length_source;
+    double max_collecting_radius;
+    double max_collecting_angle_deg;
+    double probability_additional_bias;
+    double max_relative_contribution;
+    double max_filtered_optical_depth;
+    double optical_depth_shift;
+    /* Never read from input by the reference (src/octmps.h:124); it reads
+     * an uninitialised value that is 0 in practice.  0 here. */
+    double rnd_step_size_in_tissue;
+} octmps_sim;
+
+/* ---- RNG state of one lane: the three MWC streams of init_RNG ---------- */
+typedef struct {
+    uint64_t *x;  /* general stream: step size, roulette */
+    uint32_t *a;
+    uint64_t *xR; /* reflect/transmit stream */
+    uint32_t *aR;
+    uint64_t *xS; /* spin stream */
+    uint32_t *aS;
+} octmps_rng_lanes;
+
+/* ---- one job: one A-scan (one probe position) -------------------------- */
+typedef struct {
+    octmps_mesh_id mesh;
+    const octmps_sim *sim;  /* copied at submit */
+    double probe_x, probe_y, probe_z;
+    int32_t root_tet;       /* from octmps_mesh_find_root */
+    uint64_t n_photons;     /* packets; 0 = sim->number_of_photons */
+    uint64_t seed;          /* general-stream seed (-S); 0 = 985456376 */
+    uint32_t n_lanes;       /* RNG lanes (virtual lanes) for this job; 0 = auto */
+    int32_t precision;      /* octmps_precision */
+} octmps_job;
+
+/* Tally of one job, laid out like SimState's tally arrays
+ * (src/octmps.h:155-170).  Caller-allocated arrays. */
+typedef struct {
+    uint64_t num_filtered;
+    uint64_t num_filtered_class1;
+    uint64_t num_filtered_class2;
+    uint64_t *count1; /* [nbins+1] NumClassI_PhotonsFilteredInRange */
+    uint64_t *count2; /* [nbins+1] */
+    double *sum1;     /* [nbins+2] ReflectanceClassI_Sum */
+    double *max1;     /* [nbins+2] */
+    double *sumsq1;   /* [nbins+2] */
+    double *sum2;     /* [nbins+2] ReflectanceClassII_Sum */
+    double *max2;     /* [nbins+2] */
+    double *sumsq2;   /* [nbins+2] */
+} octmps_tally;
+
+/* Per-job statistics filled by octmps_job_fetch_stats. */
+typedef struct {
+    uint64_t packets;     /* packets launched (equals n_photons) */
+    uint64_t steps;       /* propagation steps taken */
+    uint64_t restores;    /* split copies resumed */
+    double device_ms;     /* kernel time of the launch that ran the job */
+    double submit_to_done_ms;
+} octmps_job_stats;
+
+/* ---- context ------------------------------------------------------------ */
+octmps_status octmps_ctx_create(int device, octmps_ctx **out);
+octmps_status octmps_ctx_destroy(octmps_ctx *ctx);
+const char *octmps_last_error(const octmps_ctx *ctx);
+const char *octmps_status_string(octmps_status st);
+
+/* Multiplier table of the MWC generators: the first column of
+ * safeprimes_base32.txt (src/octmps_kernel.cuh:74-105).  Needed before any
+ * job is submitted; at least 3 + 3*n_lanes entries. */
+octmps_status octmps_ctx_set_multipliers(octmps_ctx *ctx, const uint32_t *a, uint64_t count);
+
+/* Launch configuration (0 = autotuned / default). */
+typedef struct {
+    int32_t block_size;       /* threads per block */
+    int32_t blocks_per_sm;    /* resident blocks per SM */
+    int32_t default_lanes;    /* RNG lanes per job when job.n_lanes = 0 */
+    int32_t use_graphs;       /* replay launches through a CUDA graph */
+    uint64_t hbm_budget_bytes;/* admission budget for job state; 0 = 80% of free */
+} octmps_launch_config;
+octmps_status octmps_ctx_configure(octmps_ctx *ctx, const octmps_launch_config *cfg);
+
+/* ---- meshes -------------------------------------------------------------- */
+octmps_status octmps_mesh_build_file(const char *path, octmps_host_mesh *out);
+void octmps_mesh_host_free(octmps_host_mesh *m);
+/* Root tet of a probe position with FindRootofGraph's rule
+ * (src/mesh.cpp:257-289); *root = -1 with OCTMPS_ERR_NOT_FOUND if the
+ * probe is not on a boundary face. */
+octmps_status octmps_mesh_find_root(const octmps_mesh_desc *m, double px, double py, double pz,
+                                    int32_t *root);
+octmps_status octmps_mesh_upload(octmps_ctx *ctx, const octmps_mesh_desc *m,
+                                 octmps_mesh_id *out);
+octmps_status octmps_mesh_release(octmps_ctx *ctx, octmps_mesh_id id);
+
+/* ---- RNG seeding (init_RNG) ---------------------------------------------- */
+octmps_status octmps_rng_init(const uint32_t *multipliers, uint64_t n_multipliers, uint32_t n_lanes,
+                              uint64_t seed, octmps_rng_lanes *out);
+
+/* ---- jobs ------------------------------------------------------------------
+ * Submitted jobs queue up; octmps_ctx_flush (or a wait on any pending job)
+ * runs every queued job in one persistent launch. */
+octmps_status octmps_job_submit(octmps_ctx *ctx, const octmps_job *job, octmps_job_id *out);
+octmps_status octmps_ctx_flush(octmps_ctx *ctx);
+octmps_status octmps_job_wait(octmps_ctx *ctx, octmps_job_id id, int32_t timeout_ms);
+octmps_status octmps_job_fetch(octmps_ctx *ctx, octmps_job_id id, octmps_tally *out);
+octmps_status octmps_job_fetch_stats(octmps_ctx *ctx, octmps_job_id id, octmps_job_stats *out);
+octmps_status octmps_job_release(octmps_ctx *ctx, octmps_job_id id);
+
+/* ---- files (the reference's formats) -------------------------------------- */
+octmps_status octmps_read_opt(const char *path, octmps_sim *out);
+octmps_status octmps_read_mci(const char *path, octmps_sim *inout);
+/* Appends one A-scan to ClassI_Scatt.out, ClassII_Scatt.out,
+ * ClassI_ScattFilt.out, ClassII_ScattFilt.out and rewrites BiasParam.mco
+ * and FilteredPhotons.mco, in directory `dir` ("" = current). */
+octmps_status octmps_write_result(const char *dir, const octmps_sim *sim, double probe_x,
+                                  const octmps_tally *t);
+
+/* ---- multiplier table generation (safeprimes_base32.txt) ---------------- */
+int octmps_safeprimes_generate(uint32_t *out, uint64_t count);
+int octmps_safeprimes_write(const char *path, uint64_t count);
+/* Reads the first column of a safe-prime file; returns entries read. */
+int64_t octmps_safeprimes_read(const char *path, uint32_t *out, uint64_t max_count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OCTMPS_CAPI_H */

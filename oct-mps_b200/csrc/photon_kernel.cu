@@ -1,0 +1,662 @@
+// The per-photon Monte Carlo hot path on sm_100a.
+//
+// One persistent kernel runs every job of a launch.  Its work unit is an RNG
+// lane of a job: a thread takes the next unit from a global counter, loads
+// that lane's three multiply-with-carry streams, and runs the lane's packets
+// one after the other (lane v of a job with N packets over V lanes runs
+// N/V packets, plus one if v < N%V), each packet to the end of its last split
+// copy.  A thread whose unit is done takes the next one, so idle lanes are
+// refilled until the launch's work runs out.  The method is the reference's
+// OCTMPSKernel loop (src/octmps_kernel.cuh:1329-1402) and the device
+// functions it calls (:475-1086), restated with the deterministic arithmetic
+// of photon_math.cuh.
+//
+// Layout the kernel reads (built by runtime.cu):
+//   planes : per tet 4 inward face planes, sign already applied
+//            (float4 x4 = 64 B per tet, or double x16 = 128 B)
+//   adj    : per tet int4 of packed neighbours (index | region << 24, or -1)
+//   regions: RegionConst<T>[n_regions] (n, mu_t, 1/mu_t, mu_a/mu_t, g)
+// The current region's constants stay in registers and are reloaded only
+// when a transmission changes region.  The split copy of a photon lives in
+// shared memory: it is written at the first biased scattering and read back
+// at the restore, a few times per packet.
+#include <cuda_runtime.h>
+
+#include "kernel_iface.h"
+#include "photon_math.cuh"
+
+namespace octmps {
+
+namespace {
+
+constexpr int kBlock = 256;
+
+template <typename T>
+struct Plane4;
+template <>
+struct Plane4<float> {
+    float v[4][4];
+    __device__ __forceinline__ void load(const void *base, int tet) {
+        const float4 *p = reinterpret_cast<const float4 *>(base) + 4 * (size_t)tet;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float4 q = __ldg(p + k);
+            v[k][0] = q.x;
+            v[k][1] = q.y;
+            v[k][2] = q.z;
+            v[k][3] = q.w;
+        }
+    }
+};
+template <>
+struct Plane4<double> {
+    double v[4][4];
+    __device__ __forceinline__ void load(const void *base, int tet) {
+        const double2 *p = reinterpret_cast<const double2 *>(base) + 8 * (size_t)tet;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const double2 a = __ldg(p + 2 * k);
+            const double2 b = __ldg(p + 2 * k + 1);
+            v[k][0] = a.x;
+            v[k][1] = a.y;
+            v[k][2] = b.x;
+            v[k][3] = b.y;
+        }
+    }
+};
+
+template <typename T, typename P>
+struct SplitCopy {
+    T x, y, z, ux, uy, uz, w, max_depth, lr;
+    P op;
+    int32_t tet, region;
+    uint32_t num_back;
+};
+
+struct PacketRecordDev {
+    unsigned long long hash, x, xR, xS;
+    uint32_t steps, hits, scatters, restores, detections, survivals;
+    double contribution, optical_path;
+};
+
+__device__ __forceinline__ unsigned long long fnv(unsigned long long h, unsigned long long v) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        h ^= (v >> (8 * i)) & 0xffull;
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+template <typename P>
+__device__ __forceinline__ void atomic_max_bits(P *addr, P v);
+template <>
+__device__ __forceinline__ void atomic_max_bits<double>(double *addr, double v) {
+    atomicMax(reinterpret_cast<unsigned long long *>(addr),
+              (unsigned long long)__double_as_longlong(v));
+}
+template <>
+__device__ __forceinline__ void atomic_max_bits<float>(float *addr, float v) {
+    atomicMax(reinterpret_cast<unsigned int *>(addr), __float_as_uint(v));
+}
+
+template <typename T, typename P, bool kRecord>
+struct Lane {
+    // photon
+    T x, y, z, ux, uy, uz, w, s, sleft, max_depth, lr, lr_after, loc_fst;
+    P op;
+    int32_t tet, region;
+    uint32_t fst_flag, num_back;
+    // current region
+    RegionConst<T> rg;
+    // generators
+    uint64_t xG, xR, xS;
+    uint32_t aG, aR, aS;
+    // job
+    const JobDesc *jd;
+    const RegionConst<T> *regions;
+    const void *planes;
+    const int4 *adj;
+    T px, py, pz;
+    int32_t type_bias;
+    // record of the current packet (kRecord only)
+    unsigned long long rhash;
+    uint32_t rsteps, rhits, rscatters, rrestores, rdetections, rsurvivals;
+    double rcontrib;
+
+    __device__ __forceinline__ T rand_co_G() { return DevNum<T>::rand_value(mwc_next(xG, aG)); }
+    __device__ __forceinline__ T rand_co_R() { return DevNum<T>::rand_value(mwc_next(xR, aR)); }
+    __device__ __forceinline__ T rand_co_S() { return DevNum<T>::rand_value(mwc_next(xS, aS)); }
+
+    __device__ __forceinline__ void load_region(int r) {
+        const T *p = reinterpret_cast<const T *>(regions + r);
+        rg.n = __ldg(p + 0);
+        rg.muas = __ldg(p + 1);
+        rg.rmuas = __ldg(p + 2);
+        rg.mua_muas = __ldg(p + 3);
+        rg.g = __ldg(p + 4);
+        region = r;
+    }
+
+    // LaunchPhoton, src/octmps_kernel.cuh:475-503.
+    __device__ __forceinline__ void launch() {
+        x = px;
+        y = py;
+        z = pz;
+        ux = 0;
+        uy = 0;
+        uz = 1;
+        w = (T)jd->w0;
+        s = 0;
+        sleft = 0;
+        op = 0;
+        max_depth = 0;
+        lr = 1;
+        lr_after = 1;
+        fst_flag = 0;
+        loc_fst = -1;
+        num_back = 0;
+        tet = jd->root_tet;
+        if (jd->root_region != region) load_region(jd->root_region);
+        if (kRecord) {
+            rhash = 14695981039346656037ull;
+            rsteps = rhits = rscatters = rrestores = rdetections = rsurvivals = 0;
+            rcontrib = 0.0;
+        }
+    }
+
+    // Class I/II tally, src/octmps_kernel.cuh:684-744.
+    __device__ void tally(T r_fresnel) {
+        const JobDesc &J = *jd;
+        const TallyLayout L = tally_layout(J.nbins, sizeof(P));
+        unsigned char *base = reinterpret_cast<unsigned char *>(J.tally);
+        unsigned long long *totals = reinterpret_cast<unsigned long long *>(base + L.totals);
+        atomicAdd(&totals[0], 1ull);
+        const P depth = DevNum<P>::div(op, (P)2);
+        const P vpf = DevNum<P>::div(depth - (P)J.shift, (P)J.bin_width);
+        long long vp;
+        if (!(vpf > (P)0)) vp = 0;
+        else if (vpf >= (P)4294967295.0) vp = 4294967295ll;
+        else vp = (long long)vpf;
+        const bool class1 = (P)max_depth > depth - (P)J.half_lc;
+        const T c = w * ((T)1 - r_fresnel) * lr;
+        const P cp = (P)c;
+        unsigned long long *cnt =
+            reinterpret_cast<unsigned long long *>(base + (class1 ? L.count1 : L.count2));
+        P *sum = reinterpret_cast<P *>(base + (class1 ? L.sum1 : L.sum2));
+        P *sumsq = reinterpret_cast<P *>(base + (class1 ? L.sumsq1 : L.sumsq2));
+        P *mx = reinterpret_cast<P *>(base + (class1 ? L.max1 : L.max2));
+        for (long long ii = vp - 3; ii < vp + 3; ++ii) {
+            if (ii >= 0 && ii < J.nbins) {
+                if (ii == vp) atomicAdd(&totals[class1 ? 1 : 2], 1ull);
+                if (kRecord) rcontrib += (double)cp;
+                atomicAdd(&sum[ii], cp);
+                atomicAdd(&sumsq[ii], cp * cp);
+                atomic_max_bits<P>(&mx[ii], cp);
+                atomicAdd(&cnt[ii], 1ull);
+            }
+        }
+    }
+
+    // SpinTheta, src/octmps_kernel.cuh:807-820.
+    __device__ __forceinline__ T spin_theta(T g) {
+        T cost;
+        if (g == (T)0) {
+            cost = (T)2 * ((T)1 - rand_co_S()) - (T)1;
+        } else {
+            const T r = (T)1 - rand_co_S();
+            const T temp = DevNum<T>::div(DevNum<T>::mad(-g, g, (T)1), DevNum<T>::mad(g + g, r, (T)1 - g));
+            cost = DevNum<T>::div(DevNum<T>::mad(-temp, temp, DevNum<T>::mad(g, g, (T)1)), g + g);
+            if (cost < (T)-1) cost = -1;
+            else if (cost > (T)1) cost = 1;
+        }
+        return cost;
+    }
+
+    // SpinThetaForwardFstBias, src/octmps_kernel.cuh:881-896.
+    __device__ __forceinline__ T spin_theta_forward(T g) {
+        T cost;
+        if (g == (T)0) {
+            cost = (T)1 - rand_co_S();
+        } else {
+            const T r = (T)1 - rand_co_S();
+            const T temp = DevNum<T>::div(r, (T)1 - g) +
+                           DevNum<T>::div((T)1 - r, sqrtT(DevNum<T>::mad(g, g, (T)1)));
+            cost = DevNum<T>::div(DevNum<T>::mad(g, g, (T)1) - DevNum<T>::div((T)1, temp * temp), g + g);
+            if (cost < (T)-1) cost = -1;
+            else if (cost > (T)1) cost = 1;
+        }
+        return cost;
+    }
+
+    // New direction from polar cosine `cost` and a drawn azimuth about
+    // (ax, ay, az) (src/octmps_kernel.cuh:844-868 and 1006-1026).
+    __device__ __forceinline__ void rotate(T cost, T ax, T ay, T az, bool copysign_form) {
+        const T sint = sqrtT(DevNum<T>::mad(-cost, cost, (T)1));
+        T sinp, cosp;
+        sincos_rand(rand_co_S(), sinp, cosp);
+        const T stcp = sint * cosp;
+        const T stsp = sint * sinp;
+        if (fabsT(az) > DevNum<T>::coszero) {
+            ux = stcp;
+            uy = stsp;
+            uz = copysign_form ? copysignT(cost, az * cost) : cost * (az >= (T)0 ? (T)1 : (T)-1);
+        } else {
+            // RSQRT(x) taken as 1/sqrt(x), both correctly rounded.
+            const T temp = rcpT(sqrtT(DevNum<T>::mad(-az, az, (T)1)));
+            ux = DevNum<T>::mad(DevNum<T>::mad(stcp * ax, az, -(stsp * ay)), temp, ax * cost);
+            uy = DevNum<T>::mad(DevNum<T>::mad(stcp * ay, az, stsp * ax), temp, ay * cost);
+            uz = DevNum<T>::mad(az, cost, DevNum<T>::div(-stcp, temp));
+        }
+    }
+
+    // SpinBias, src/octmps_kernel.cuh:898-1086.
+    __device__ void spin_bias(SplitCopy<T, P> &cont) {
+        const JobDesc &J = *jd;
+        const T g = rg.g;
+        const T g2 = g * g;
+        T ax = ux, ay = uy, az = uz;
+        const T ox = ux, oy = uy, oz = uz;
+        T btmp = 0;
+        int reached = 0;
+        bool first = false;
+        if (z > (T)J.tdmin && z < (T)J.tdmax && uz > (T)0 && !fst_flag) {
+            cont.x = x;
+            cont.y = y;
+            cont.z = z;
+            cont.ux = ux;
+            cont.uy = uy;
+            cont.uz = uz;
+            cont.w = w;
+            cont.max_depth = max_depth;
+            cont.lr = lr;
+            cont.op = op;
+            cont.tet = tet;
+            cont.region = region;
+            cont.num_back = num_back;
+            reached = 1;
+            fst_flag = 1;
+            loc_fst = z;
+            btmp = (T)J.bias_a;
+            first = true;
+        }
+        T vx = px - x;
+        T vy = py - y;
+        T vz = pz - z;
+        const T len = sqrtT(DevNum<T>::mad(vz, vz, DevNum<T>::mad(vx, vx, vy * vy)));
+        vx = DevNum<T>::div(vx, len);
+        vy = DevNum<T>::div(vy, len);
+        vz = DevNum<T>::div(vz, len);
+        if ((fst_flag || num_back > 0) && !reached) {
+            reached = 2;
+            const T next_step = DevNum<T>::div(-log_method((T)J.rnd_step), rg.muas);
+            if (next_step >= len && -vz >= (T)J.cos_collect) reached = 1;
+            btmp = (T)J.bias_a;
+        }
+        int sel = 0;
+        T cost;
+        const T pb = (T)J.p_bias;
+        if (reached) {
+            sel = rand_co_S() <= pb ? 1 : 2;
+            if (reached == 1 || sel == 1) {
+                cost = spin_theta_forward(btmp);
+                ax = vx;
+                ay = vy;
+                az = vz;
+            } else {
+                cost = spin_theta(g);
+            }
+        } else {
+            cost = spin_theta(g);
+        }
+        cost = fmaxT(cost, (T)-1);
+        cost = fminT(cost, (T)1);
+        rotate(cost, ax, ay, az, true);
+
+        const T costg = dot3<T>(ox, oy, oz, ux, uy, uz);
+        const T costg1 = dot3<T>(vx, vy, vz, ux, uy, uz);
+        if (btmp != (T)0) {
+            const T opa2 = DevNum<T>::mad(btmp, btmp, (T)1);
+            const T sq_opa2 = sqrtT(opa2);
+            T f;
+            if (reached == 1) {
+                const T b1 = opa2 - (btmp + btmp) * cost;
+                const T h1 = DevNum<T>::mad(g, g, (T)1) - (g + g) * costg;
+                const T num = ((T)1 - g2) * (sq_opa2 - (T)1 + btmp) * sqrtT(b1 * b1 * b1);
+                const T den = (btmp + btmp) * ((T)1 - btmp) * sq_opa2 * sqrtT(h1 * h1 * h1);
+                f = DevNum<T>::div(num, den);
+            } else {
+                const T c1 = sel == 1 ? cost : costg1;
+                const T c2 = sel == 1 ? costg : cost;
+                const T b1 = opa2 - (btmp + btmp) * c1;
+                const T pdf1 = DevNum<T>::div(sq_opa2 * btmp * ((T)1 - btmp),
+                                              (sq_opa2 - (T)1 + btmp) * sqrtT(b1 * b1 * b1));
+                const T h2 = sqrtT(DevNum<T>::mad(g, g, (T)1) - (g + g) * c2);
+                const T pdf2 = DevNum<T>::div((T)1 - g2, (T)2 * (h2 * h2 * h2));
+                f = DevNum<T>::div(pdf2, DevNum<T>::mad(pb, pdf1, ((T)1 - pb) * pdf2));
+            }
+            lr *= f;
+            if (first) lr_after = lr;
+        }
+    }
+
+    // One propagation step: OCTMPSKernel's loop body
+    // (src/octmps_kernel.cuh:1351-1392).  Returns true when the packet ends.
+    __device__ __forceinline__ bool step(SplitCopy<T, P> &cont, unsigned int *err) {
+        int ev = 0;
+        // ComputeStepSize, :505-515
+        if (sleft == (T)0) {
+            const T r = (T)1 - rand_co_G();
+            s = -log_method(r) * rg.rmuas;
+        } else {
+            s = sleft * rg.rmuas;
+            sleft = 0;
+        }
+        // HitBoundary, :517-572
+        Plane4<T> pl;
+        pl.load(planes, tet);
+        const int4 nb = __ldg(adj + tet);
+        T cosv[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) cosv[k] = dot3<T>(pl.v[k][0], pl.v[k][1], pl.v[k][2], ux, uy, uz);
+        T min_d = DevNum<T>::big;
+        T min_cos = 0;
+        int face = -1;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (cosv[k] < (T)0) {
+                const T perp = dot3<T>(pl.v[k][0], pl.v[k][1], pl.v[k][2], x, y, z) + pl.v[k][3];
+                const T t = DevNum<T>::div(-perp, cosv[k]);
+                if (t < min_d) {
+                    min_d = t;
+                    face = k;
+                    min_cos = cosv[k];
+                }
+            }
+        }
+        const bool hit = s > min_d;
+        if (hit) {
+            sleft = (s - min_d) * rg.muas;
+            s = min_d;
+        }
+        // Hop, :574-582
+        x = DevNum<T>::mad(s, ux, x);
+        y = DevNum<T>::mad(s, uy, y);
+        z = DevNum<T>::mad(s, uz, z);
+        op += (P)s;
+        if (max_depth < z) max_depth = z;
+
+        if (hit) {
+            if (face < 0) {
+                atomicOr(err, kErrNoExitFace);
+                return true;
+            }
+            // FastReflectTransmit, :590-775
+            if (kRecord) ++rhits;
+            const T ca1 = -min_cos;
+            const int32_t entry = face == 0 ? nb.x : face == 1 ? nb.y : face == 2 ? nb.z : nb.w;
+            const int next_region = entry < 0 ? 0 : (int)((uint32_t)entry >> kAdjIndexBits);
+            const T nt = entry < 0 ? (T)jd->n_ambient
+                                   : __ldg(reinterpret_cast<const T *>(regions + next_region));
+            const T ni_nt = DevNum<T>::div(rg.n, nt);
+            T sa1 = sqrtT(DevNum<T>::mad(-ca1, ca1, (T)1));
+            if (ca1 > DevNum<T>::coszero) sa1 = 0;
+            const T sa2 = fminT(ni_nt * sa1, (T)1);
+            const T ca2 = sqrtT(DevNum<T>::mad(-sa2, sa2, (T)1));
+            const T ca1ca2 = ca1 * ca2;
+            const T sa1sa2 = sa1 * sa2;
+            T sa1ca2 = sa1 * ca2;
+            T ca1sa2 = ca1 * sa2;
+            if (ca1 > DevNum<T>::coszero) {
+                sa1ca2 = 1;
+                ca1sa2 = ni_nt;
+            }
+            const T cam = ca1ca2 + sa1sa2;
+            const T sap = sa1ca2 + ca1sa2;
+            const T sam = sa1ca2 - ca1sa2;
+            T r = DevNum<T>::div(sam, sap * cam);
+            r = r * r;
+            r = r * DevNum<T>::mad(ca1ca2, ca1ca2, sa1sa2 * sa1sa2);
+            if (ca1 < DevNum<T>::cos90 || sa2 == (T)1) r = 1;
+
+            const T fnx = face == 0 ? pl.v[0][0] : face == 1 ? pl.v[1][0] : face == 2 ? pl.v[2][0] : pl.v[3][0];
+            const T fny = face == 0 ? pl.v[0][1] : face == 1 ? pl.v[1][1] : face == 2 ? pl.v[2][1] : pl.v[3][1];
+            const T fnz = face == 0 ? pl.v[0][2] : face == 1 ? pl.v[1][2] : face == 2 ? pl.v[2][2] : pl.v[3][2];
+            const T two_ca1 = ca1 + ca1;
+            const T rx = DevNum<T>::mad(two_ca1, fnx, ux);
+            const T ry = DevNum<T>::mad(two_ca1, fny, uy);
+            const T rz = DevNum<T>::mad(two_ca1, fnz, uz);
+            const T rnd = rand_co_R();
+            if (entry < 0 && r < (T)1) {
+                ev = 4;
+                if (uz < (T)0) {
+                    bool filt = false;
+                    const T dx = x - px;
+                    const T dy = y - py;
+                    const T rr = sqrtT(DevNum<T>::mad(dx, dx, dy * dy));
+                    if (rr < (T)jd->radius && -uz > (T)jd->cos_collect) {
+                        if (type_bias == 0 || type_bias == 3) filt = true;
+                        if ((fst_flag && type_bias == 37) || (loc_fst == max_depth && type_bias != 37) ||
+                            num_back > 0)
+                            filt = true;
+                    }
+                    if (filt) {
+                        tally(r);
+                        ev |= 8;
+                        if (kRecord) ++rdetections;
+                    }
+                } else {
+                    num_back++;
+                }
+                w *= r;
+                ux = rx;
+                uy = ry;
+                uz = rz;
+            } else if (rnd > r) {
+                const int next = (int)((uint32_t)entry & kAdjIndexMask);
+                tet = next;
+                if (next_region != region) load_region(next_region);
+                ev = 2;
+            } else {
+                if (uz > (T)0) num_back++;
+                ux = rx;
+                uy = ry;
+                uz = rz;
+                ev = 3;
+            }
+        } else {
+            ev = 1;
+            if (kRecord) ++rscatters;
+            // Drop, :584-588
+            w = DevNum<T>::mad(-w, rg.mua_muas, w);
+            if (type_bias == 0) {
+                rotate(spin_theta(rg.g), ux, uy, uz, false);
+            } else if (type_bias == 37) {
+                spin_bias(cont);
+            }
+        }
+        // Roulette, :1376-1392
+        bool end = false;
+        if (w < DevNum<T>::weight) {
+            const T rnd = rand_co_G();
+            if (w != (T)0 && rnd < DevNum<T>::chance) {
+                w *= DevNum<T>::div((T)1, DevNum<T>::chance);
+                ev |= 16;
+                if (kRecord) ++rsurvivals;
+            } else if (fst_flag && type_bias != 3) {
+                const T lr_tmp = lr_after;
+                x = cont.x;
+                y = cont.y;
+                z = cont.z;
+                ux = cont.ux;
+                uy = cont.uy;
+                uz = cont.uz;
+                w = cont.w;
+                max_depth = cont.max_depth;
+                lr = cont.lr;
+                op = cont.op;
+                tet = cont.tet;
+                num_back = cont.num_back;
+                fst_flag = 0;
+                loc_fst = -1;
+                sleft = 0;
+                if (cont.region != region) load_region(cont.region);
+                rotate(spin_theta(rg.g), ux, uy, uz, false);
+                lr = lr_tmp < (T)1 ? (T)1 - lr_tmp : (T)1;
+                ev |= 32;
+                if (kRecord) ++rrestores;
+                restores_++;
+            } else {
+                ev |= 64;
+                end = true;
+            }
+        }
+        if (kRecord) {
+            rhash = fnv(rhash, ((unsigned long long)(uint32_t)tet << 8) | (unsigned long long)ev);
+            ++rsteps;
+        }
+        return end;
+    }
+    uint32_t restores_;
+};
+
+template <typename T, typename P, bool kRecord>
+__global__ void __launch_bounds__(kBlock)
+    photon_kernel(const LaunchArgs args, PacketRecordDev *records) {
+    __shared__ SplitCopy<T, P> cont_all[kBlock];
+    SplitCopy<T, P> &cont = cont_all[threadIdx.x];
+    Lane<T, P, kRecord> L;
+    L.jd = nullptr;
+    L.region = -1;
+    L.restores_ = 0;
+    uint64_t packets_left = 0, steps_packet = 0, steps_unit = 0, packets_unit = 0, capped = 0;
+    uint64_t record_lane = ~0ull;  // lane whose first packet is being recorded
+    bool recording = false;
+
+    for (;;) {
+        if (packets_left == 0) {
+            if (L.jd) {
+                atomicAdd(&L.jd->stats[0], (unsigned long long)steps_unit);
+                atomicAdd(&L.jd->stats[1], (unsigned long long)L.restores_);
+                atomicAdd(&L.jd->stats[2], (unsigned long long)packets_unit);
+                if (capped) atomicAdd(&L.jd->stats[3], (unsigned long long)capped);
+            }
+            steps_unit = packets_unit = capped = 0;
+            L.restores_ = 0;
+            const unsigned long long u = atomicAdd(args.next_unit, 1ull);
+            if (u >= args.total_units) break;
+            int lo = 0, hi = args.n_jobs - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (__ldg(args.unit_base + mid) <= u) lo = mid;
+                else hi = mid - 1;
+            }
+            const JobDesc *jd = args.jobs + lo;
+            const uint64_t v = u - __ldg(args.unit_base + lo);
+            if (jd != L.jd) {
+                L.jd = jd;
+                L.regions = reinterpret_cast<const RegionConst<T> *>(jd->regions);
+                L.planes = jd->planes;
+                L.adj = reinterpret_cast<const int4 *>(jd->adj);
+                L.px = (T)jd->probe_x;
+                L.py = (T)jd->probe_y;
+                L.pz = (T)jd->probe_z;
+                L.type_bias = jd->type_bias;
+                L.region = -1;
+            }
+            L.xG = jd->rng_x[v];
+            L.aG = jd->rng_a[v];
+            L.xR = jd->rng_xR[v];
+            L.aR = jd->rng_aR[v];
+            L.xS = jd->rng_xS[v];
+            L.aS = jd->rng_aS[v];
+            const uint64_t nl = jd->n_lanes;
+            packets_left = jd->n_photons / nl + (v < jd->n_photons % nl ? 1 : 0);
+            if (packets_left == 0) continue;
+            L.launch();
+            steps_packet = 0;
+            recording = kRecord && records && lo == 0;
+            record_lane = v;
+        }
+        const bool end = L.step(cont, args.error);
+        ++steps_packet;
+        bool done = end;
+        if (!done && steps_packet >= args.step_cap) {
+            atomicOr(args.error, kErrStepCap);
+            ++capped;
+            done = true;
+        }
+        if (done) {
+            steps_unit += steps_packet;
+            ++packets_unit;
+            if (kRecord && recording) {
+                PacketRecordDev r;
+                r.hash = L.rhash;
+                r.x = L.xG;
+                r.xR = L.xR;
+                r.xS = L.xS;
+                r.steps = L.rsteps;
+                r.hits = L.rhits;
+                r.scatters = L.rscatters;
+                r.restores = L.rrestores;
+                r.detections = L.rdetections;
+                r.survivals = L.rsurvivals;
+                r.contribution = L.rcontrib;
+                r.optical_path = (double)L.op;
+                records[record_lane] = r;
+                recording = false;
+            }
+            --packets_left;
+            if (packets_left) {
+                L.launch();
+                steps_packet = 0;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+int launch_photon_kernel(int precision, const LaunchArgs &args, int grid, int block, void *stream,
+                         void *records) {
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    PacketRecordDev *rec = reinterpret_cast<PacketRecordDev *>(records);
+    if (block != kBlock) return (int)cudaErrorInvalidValue;
+    if (rec) {
+        switch (precision) {
+            case kMixed: photon_kernel<float, double, true><<<grid, block, 0, st>>>(args, rec); break;
+            case kFP32: photon_kernel<float, float, true><<<grid, block, 0, st>>>(args, rec); break;
+            case kFP64: photon_kernel<double, double, true><<<grid, block, 0, st>>>(args, rec); break;
+            default: return (int)cudaErrorInvalidValue;
+        }
+    } else {
+        switch (precision) {
+            case kMixed: photon_kernel<float, double, false><<<grid, block, 0, st>>>(args, nullptr); break;
+            case kFP32: photon_kernel<float, float, false><<<grid, block, 0, st>>>(args, nullptr); break;
+            case kFP64: photon_kernel<double, double, false><<<grid, block, 0, st>>>(args, nullptr); break;
+            default: return (int)cudaErrorInvalidValue;
+        }
+    }
+    return (int)cudaGetLastError();
+}
+
+int photon_kernel_attributes(int precision, int block, int *regs, int *max_blocks_per_sm) {
+    cudaFuncAttributes a;
+    const void *fn = nullptr;
+    switch (precision) {
+        case kMixed: fn = (const void *)photon_kernel<float, double, false>; break;
+        case kFP32: fn = (const void *)photon_kernel<float, float, false>; break;
+        case kFP64: fn = (const void *)photon_kernel<double, double, false>; break;
+        default: return (int)cudaErrorInvalidValue;
+    }
+    cudaError_t e = cudaFuncGetAttributes(&a, fn);
+    if (e != cudaSuccess) return (int)e;
+    *regs = a.numRegs;
+    int nb = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, block, 0);
+    if (e != cudaSuccess) return (int)e;
+    *max_blocks_per_sm = nb;
+    return 0;
+}
+
+}  // namespace octmps

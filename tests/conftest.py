@@ -1,0 +1,100 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+REF_INPUT = "/root/reference/input"
+sys.path.insert(0, os.path.join(ROOT, "oct-mps_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs an sm_100 GPU (run with -m gpu)")
+
+
+@pytest.fixture(scope="session")
+def octmps():
+    import octmps as m
+    return m
+
+
+@pytest.fixture(scope="session")
+def meshgen():
+    import meshgen as m
+    return m
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    import oracle_py
+    return oracle_py.Oracle()
+
+
+@pytest.fixture(scope="session")
+def reference():
+    import oracle_py
+    try:
+        return oracle_py.Reference()
+    except ImportError as e:
+        pytest.skip(f"reference host build unavailable: {e}")
+
+
+@pytest.fixture(scope="session")
+def workdir(tmp_path_factory):
+    return str(tmp_path_factory.mktemp("octmps"))
+
+
+@pytest.fixture(scope="session")
+def multipliers(octmps):
+    """The generated multiplier table (the reference's safe-prime list is not shipped)."""
+    return octmps.safeprimes(3 + 3 * 30000)
+
+
+@pytest.fixture(scope="session")
+def small_deck(octmps, meshgen, workdir):
+    p = meshgen.config_small(os.path.join(workdir, "small"), n_photons=20000)
+    sim = octmps.read_deck(p["opt"], p["mci"])
+    mesh = octmps.build_mesh(p["mesh"])
+    root = mesh.find_root(sim.start_x)
+    return {"paths": p, "sim": sim, "mesh": mesh, "root": root}
+
+
+@pytest.fixture(scope="session")
+def small_matched_deck(octmps, meshgen, workdir):
+    p = meshgen.config_small(os.path.join(workdir, "small_matched"), n_photons=20000, matched=True)
+    sim = octmps.read_deck(p["opt"], p["mci"])
+    mesh = octmps.build_mesh(p["mesh"])
+    root = mesh.find_root(sim.start_x)
+    return {"paths": p, "sim": sim, "mesh": mesh, "root": root}
+
+
+def ref_deck_paths(name):
+    import json
+    decks = json.load(open(os.path.join(GOLDEN, "decks.json")))
+    files = decks[name]["files"]
+    paths = [os.path.join(REF_INPUT, f) for f in files]
+    if not all(os.path.exists(p) for p in paths):
+        pytest.skip("reference input decks not present")
+    return paths
+
+
+def three_sigma_ok(sum_a, sumsq_a, n_a, sum_b, sumsq_b, n_b, k=3.0, min_count=None, counts=None):
+    """Per-bin agreement of two Monte Carlo means within k combined standard errors.
+
+    Mean and standard error per bin as the reference's writer computes them
+    (src/octmps_io.cpp:310-318): mean = Sum/N, var = (SumSq/N - mean^2)/(N-1).
+    Returns (fraction of bins within k sigma, worst |z|)."""
+    ma, mb = sum_a / n_a, sum_b / n_b
+    va = np.maximum(sumsq_a / n_a - ma * ma, 0) / (n_a - 1)
+    vb = np.maximum(sumsq_b / n_b - mb * mb, 0) / (n_b - 1)
+    se = np.sqrt(va + vb)
+    sel = se > 0
+    if counts is not None and min_count is not None:
+        sel &= counts >= min_count
+    z = np.abs(ma - mb)[sel] / se[sel]
+    if len(z) == 0:
+        return 1.0, 0.0
+    return float(np.mean(z <= k)), float(np.max(z))

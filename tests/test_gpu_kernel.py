@@ -1,0 +1,229 @@
+"""The CUDA photon kernel against the CPU oracle, through the C-ABI.
+
+Bit-exact: every packet's event sequence (tet and event kind per step), its
+generator states at the end, its step/hit/scatter/restore/detection counts,
+its optical path and summed contribution, in each precision; every tally
+count.  Tally sums agree to summation order only (device atomics): 1e-12
+relative in FP64 accumulation, 1e-5 in the all-FP32 form.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT, three_sigma_ok
+
+import oracle_py
+
+pytestmark = pytest.mark.gpu
+
+REC_BYTES = oracle_py.PACKET_DTYPE.itemsize
+SUM_RTOL = {0: 1e-12, 1: 1e-5, 2: 1e-12}
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.fail("a GPU test ran without a CUDA device")
+    return torch
+
+
+@pytest.fixture(scope="module")
+def ctx(octmps, multipliers, torch_cuda):
+    c = octmps.Context(0, multipliers)
+    yield c
+    c.close()
+
+
+def run_gpu(ctx, torch, deck, n_photons, lanes, seed, precision, record=True):
+    mid = ctx.upload_mesh(deck["mesh"])
+    sim = deck["sim"]
+    buf = torch.zeros(lanes * REC_BYTES, dtype=torch.uint8, device="cuda") if record else None
+    jid = ctx.submit(mid, sim, sim.start_x, deck["root"], n_photons=n_photons, seed=seed,
+                     n_lanes=lanes, precision=precision)
+    if record:
+        ctx.record_next_launch(buf.data_ptr())
+    ctx.flush()
+    t = ctx.fetch(jid, sim.num_optical_depth_length_steps)
+    st = ctx.stats(jid)
+    ctx.release(jid)
+    ctx.release_mesh(mid)
+    rec = np.frombuffer(buf.cpu().numpy().tobytes(), dtype=oracle_py.PACKET_DTYPE) if record else None
+    return t, st, rec
+
+
+def run_oracle(oracle, octmps, deck, n_photons, lanes, seed, precision, multipliers):
+    rng = octmps.rng_init(multipliers[: 3 + 3 * lanes], lanes, seed)
+    p = oracle_py.params_from_sim(deck["sim"])
+    return oracle.run(p, deck["mesh"], (deck["sim"].start_x, 0, 0), deck["root"], n_photons,
+                      lanes, rng, precision, record=True)
+
+
+def assert_tallies_equal(t_gpu, t_orc, precision, nbins):
+    for k in ("num_filtered", "num_filtered_class1", "num_filtered_class2"):
+        assert t_gpu[k] == t_orc[k], k
+    for k in ("count1", "count2"):
+        np.testing.assert_array_equal(t_gpu[k], t_orc[k], err_msg=k)
+    for k in ("sum1", "sumsq1", "sum2", "sumsq2"):
+        np.testing.assert_allclose(t_gpu[k][:nbins], t_orc[k][:nbins], rtol=SUM_RTOL[precision],
+                                   atol=0, err_msg=k)
+    for k in ("max1", "max2"):
+        np.testing.assert_array_equal(t_gpu[k][:nbins], t_orc[k][:nbins], err_msg=k)
+
+
+def assert_records_equal(r_gpu, r_orc):
+    for f in r_orc.dtype.names:
+        bad = np.where(r_gpu[f] != r_orc[f])[0]
+        assert len(bad) == 0, (f, bad[:5], r_gpu[f][bad[:3]], r_orc[f][bad[:3]])
+
+
+@pytest.mark.parametrize("precision", [0, 1, 2])
+@pytest.mark.parametrize("deckname", ["small_deck", "small_matched_deck"])
+def test_first_packets_and_tallies_bit_exact(request, ctx, torch_cuda, octmps, oracle,
+                                             multipliers, precision, deckname):
+    deck = request.getfixturevalue(deckname)
+    lanes, n = 3000, 3000  # one packet per lane
+    t_g, st, r_g = run_gpu(ctx, torch_cuda, deck, n, lanes, 985456376, precision)
+    t_o, r_o = run_oracle(oracle, octmps, deck, n, lanes, 985456376, precision, multipliers)
+    assert st["packets"] == n
+    assert st["steps"] == t_o["steps"] and st["restores"] == t_o["restores"]
+    assert_records_equal(r_g, r_o)
+    assert_tallies_equal(t_g, t_o, precision, deck["sim"].num_optical_depth_length_steps)
+
+
+@pytest.mark.parametrize("precision", [0, 2])
+def test_many_packets_per_lane_bit_exact(ctx, torch_cuda, octmps, oracle, multipliers, small_deck,
+                                         precision):
+    """Lanes run several packets in a row from the same streams (N % lanes != 0)."""
+    lanes, n = 997, 20000
+    t_g, st, r_g = run_gpu(ctx, torch_cuda, small_deck, n, lanes, 5, precision)
+    t_o, r_o = run_oracle(oracle, octmps, small_deck, n, lanes, 5, precision, multipliers)
+    assert st["packets"] == n and st["steps"] == t_o["steps"]
+    assert_records_equal(r_g, r_o)
+    assert_tallies_equal(t_g, t_o, precision, small_deck["sim"].num_optical_depth_length_steps)
+
+
+def test_batch_equals_alone(ctx, torch_cuda, octmps, small_deck, small_matched_deck):
+    """Jobs of two meshes, several probes, seeds and sizes in one persistent
+    launch give the same counts as each job alone (sums to summation order)."""
+    specs = [(small_deck, 0.0, 1, 5000, 1000), (small_matched_deck, 0.0, 2, 3000, 3000),
+             (small_deck, 0.0, 3, 8000, 777), (small_matched_deck, 0.0, 4, 100, 100)]
+    meshes = {id(d): ctx.upload_mesh(d["mesh"]) for d, *_ in specs}
+    nb = small_deck["sim"].num_optical_depth_length_steps
+    alone = []
+    for d, x, seed, n, lanes in specs:
+        j = ctx.submit(meshes[id(d)], d["sim"], x, d["root"], n_photons=n, seed=seed, n_lanes=lanes)
+        alone.append(ctx.fetch(j, nb))
+        ctx.release(j)
+    ids = [ctx.submit(meshes[id(d)], d["sim"], x, d["root"], n_photons=n, seed=seed, n_lanes=lanes)
+           for d, x, seed, n, lanes in specs]
+    ctx.flush()
+    for j, a, s in zip(ids, alone, specs):
+        b = ctx.fetch(j, nb)
+        assert ctx.stats(j)["packets"] == s[3]
+        assert_tallies_equal(b, a, 0, nb)
+        ctx.release(j)
+    for mid in meshes.values():
+        ctx.release_mesh(mid)
+
+
+def test_product_form_within_3_sigma_of_reference(ctx, octmps, small_deck):
+    """The default (mixed FP32/FP64) kernel against four reference A-scans."""
+    ref = np.load(os.path.join(GOLDEN, "small_ref_tallies.npz"))
+    sim = small_deck["sim"]
+    nb = sim.num_optical_depth_length_steps
+    n = sim.number_of_photons
+    mid = ctx.upload_mesh(small_deck["mesh"])
+    ids = [ctx.submit(mid, sim, sim.start_x, small_deck["root"], seed=s, n_lanes=2400)
+           for s in (21, 22, 23, 24)]
+    ts = [ctx.fetch(j, nb) for j in ids]
+    for j in ids:
+        ctx.release(j)
+    ctx.release_mesh(mid)
+    g = {k: sum(t[k] for t in ts) for k in ("sum1", "sumsq1", "sum2", "sumsq2")}
+    r = {k: sum(ref[f"run{i}_{k}"] for i in range(4)) for k in g}
+    for c in ("1", "2"):
+        frac, worst = three_sigma_ok(g["sum" + c][:nb], g["sumsq" + c][:nb], 4 * n,
+                                     r["sum" + c][:nb], r["sumsq" + c][:nb], 4 * n)
+        assert frac >= 0.98 and worst < 6.0, (c, frac, worst)
+
+
+def test_full_size_plain_ascan(ctx, torch_cuda, octmps, oracle, meshgen, multipliers, workdir):
+    """Config 1 at full size (288,000 tets, 1e5 packets, one A-scan): the first
+    packets of 2000 lanes bit-exact against the oracle; whole-run invariants."""
+    p = meshgen.config_plain_ascan(os.path.join(workdir, "plain"))
+    sim = octmps.read_deck(p["opt"], p["mci"])
+    deck = {"sim": sim, "mesh": octmps.build_mesh(p["mesh"]), "root": None}
+    deck["root"] = deck["mesh"].find_root(sim.start_x)
+    t_g, st, r_g = run_gpu(ctx, torch_cuda, deck, 2000, 2000, 1, 0)
+    t_o, r_o = run_oracle(oracle, octmps, deck, 2000, 2000, 1, 0, multipliers)
+    assert_records_equal(r_g, r_o)
+    assert_tallies_equal(t_g, t_o, 0, sim.num_optical_depth_length_steps)
+    mid = ctx.upload_mesh(deck["mesh"])
+    j = ctx.submit(mid, sim, sim.start_x, deck["root"], seed=1)
+    t = ctx.fetch(j, sim.num_optical_depth_length_steps)
+    s = ctx.stats(j)
+    ctx.release(j)
+    ctx.release_mesh(mid)
+    assert s["packets"] == 100000
+    assert t["num_filtered"] > 0
+    # every detection adds one count to each in-range bin of its window of 6
+    assert t["count1"].sum() + t["count2"].sum() <= 6 * t["num_filtered"]
+    assert t["num_filtered_class1"] + t["num_filtered_class2"] <= t["num_filtered"]
+    assert np.all(t["max1"] <= t["sum1"] + 1e-300) and np.all(t["sumsq1"] >= 0)
+
+
+def test_error_paths(ctx, octmps, small_deck):
+    sim = small_deck["sim"]
+    mid = ctx.upload_mesh(small_deck["mesh"])
+    with pytest.raises(octmps.OctmpsError) as e:
+        ctx.submit(mid, sim, 0.0, -1)
+    assert e.value.status == 1
+    with pytest.raises(octmps.OctmpsError) as e:
+        ctx.submit(mid + 1000, sim, 0.0, small_deck["root"])
+    assert e.value.status == 5
+    with pytest.raises(octmps.OctmpsError) as e:
+        ctx.submit(mid, sim, 0.0, small_deck["root"], precision=7)
+    assert e.value.status == 1
+    with pytest.raises(octmps.OctmpsError) as e:
+        ctx.submit(mid, sim, 0.0, small_deck["root"], n_photons=10 ** 6, n_lanes=10 ** 6)
+    assert e.value.status == 1
+    # a wait that times out leaves the job running; a later wait completes it
+    j = ctx.submit(mid, sim, 0.0, small_deck["root"], n_photons=400000, n_lanes=4000)
+    ctx.flush()
+    st = ctx.wait(j, 0)
+    assert st in (0, 4)
+    assert ctx.wait(j, -1) == 0
+    ctx.release(j)
+    ctx.release_mesh(mid)
+    with pytest.raises(octmps.OctmpsError):
+        ctx.release_mesh(mid)
+
+
+def test_cli_end_to_end(octmps, oracle, small_deck, multipliers, tmp_path):
+    """The drop-in CLI writes the reference's four .out files; its counts equal
+    the oracle's for the same lanes and seed, its means to print precision."""
+    p = small_deck["paths"]
+    np.savetxt(tmp_path / "safeprimes_base32.txt",
+               np.stack([multipliers, multipliers - 1, np.full_like(multipliers, 2 ** 32 - 1)], 1),
+               fmt="%d")
+    exe = os.path.join(ROOT, "oct-mps_b200", "octmps")
+    r = subprocess.run([exe, "-S7", "-L2400", p["opt"], p["mesh"], p["mci"]], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    sim = small_deck["sim"]
+    rng = octmps.rng_init(multipliers[: 3 + 3 * 2400], 2400, 7)
+    t = oracle.run(oracle_py.params_from_sim(sim), small_deck["mesh"], (sim.start_x, 0, 0),
+                   small_deck["root"], sim.number_of_photons, 2400, rng, 0)
+    d = tmp_path / "want"
+    d.mkdir()
+    octmps.write_result(str(d), sim, sim.start_x, t)
+    for fn in ("ClassI_Scatt.out", "ClassII_Scatt.out", "ClassI_ScattFilt.out",
+               "ClassII_ScattFilt.out"):
+        got = np.loadtxt(tmp_path / fn, delimiter=",")
+        want = np.loadtxt(d / fn, delimiter=",")
+        np.testing.assert_array_equal(got[:, [0, 1, 4]], want[:, [0, 1, 4]])
+        np.testing.assert_allclose(got[:, 2:4], want[:, 2:4], rtol=2e-5, atol=0)
+    assert (tmp_path / "BiasParam.mco").read_text() == (d / "BiasParam.mco").read_text()

@@ -1,0 +1,160 @@
+"""The CPU oracle (oracle/oracle.cpp) pinned against the reference's own code.
+
+* its math kernels against numpy in float64 (error bounds),
+* its FP64 first-packet event sequences against the reference routine's on
+  the Sphere deck (tests/golden/sphere_first_packets.npz),
+* its per-bin Class I/II tallies, in all three precisions, against full
+  A-scans of the reference routine (tests/golden/small_ref_tallies.npz)
+  within 3 standard errors.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ref_deck_paths, three_sigma_ok
+
+import oracle_py
+
+
+def ulp32(x):
+    return np.spacing(np.abs(np.float32(x))).astype(np.float64)
+
+
+def test_logf_accuracy(oracle):
+    rng = np.random.default_rng(1)
+    xs = np.concatenate([rng.random(20000), np.float32(2.0) ** -np.arange(1, 25), [1.0]])
+    xs = xs[xs > 0].astype(np.float32)
+    got = np.array([oracle.L.oracle_logf(float(x)) for x in xs], np.float64)
+    want = np.log(xs.astype(np.float64))
+    err = np.abs(got - want) / np.maximum(ulp32(want), np.spacing(np.float32(0.5)) * 1e-30)
+    assert np.max(err[want != 0]) <= 2.0
+    assert oracle.L.oracle_logf(1.0) == 0.0
+    assert oracle.L.oracle_logf(0.0) == -np.inf
+
+
+def test_log_accuracy(oracle):
+    rng = np.random.default_rng(2)
+    xs = np.concatenate([rng.random(20000), 2.0 ** -np.arange(1, 60), rng.random(100) * 1e6])
+    xs = xs[xs > 0]
+    got = np.array([oracle.L.oracle_log(float(x)) for x in xs])
+    want = np.log(xs)
+    err = np.abs(got - want) / np.spacing(np.abs(want))
+    assert np.max(err[want != 0]) <= 2.0
+    assert oracle.L.oracle_log(0.0) == -np.inf
+
+
+def test_sincos_accuracy(oracle):
+    rng = np.random.default_rng(3)
+    u = rng.integers(0, 2 ** 32, 20000, dtype=np.uint64)
+    t = np.array([oracle.L.oracle_uint2float_rz(int(v)) for v in u], np.float64) * 2.0 ** -32
+    s, c = C.c_float(), C.c_float()
+    sd, cd = C.c_double(), C.c_double()
+    es, ed = [], []
+    for tv in t:
+        oracle.L.oracle_sincos_turn_f(float(tv), C.byref(s), C.byref(c))
+        es.append(max(abs(s.value - np.sin(2 * np.pi * tv)), abs(c.value - np.cos(2 * np.pi * tv))))
+        psi = (2.0 * 3.14159265359) * tv
+        oracle.L.oracle_sincos_d(psi, C.byref(sd), C.byref(cd))
+        ed.append(max(abs(sd.value - np.sin(psi)), abs(cd.value - np.cos(psi))))
+    assert max(es) < 2.5e-7  # about 4 float ulps of 1
+    assert max(ed) < 5e-16
+
+
+def test_div_rd_and_rz_conversion(oracle):
+    from fractions import Fraction
+    rng = np.random.default_rng(4)
+    for a, b in zip(rng.normal(size=2000), rng.normal(size=2000)):
+        q = oracle.L.oracle_div_rd(a, b)
+        assert Fraction(q) <= Fraction(a) / Fraction(b) < Fraction(np.nextafter(q, np.inf))
+    assert oracle.L.oracle_div_rd(1.0, 0.1) == np.nextafter(10.0, 0.0)
+    for u in rng.integers(0, 2 ** 32, 5000, dtype=np.uint64):
+        f = oracle.L.oracle_uint2float_rz(int(u))
+        assert f <= int(u) < float(np.nextafter(np.float32(f), np.float32(np.inf)))
+
+
+def first_packet_match(oracle, octmps, name="Sphere"):
+    opt, mesh_path, mci = ref_deck_paths(name)
+    fix = np.load(os.path.join(GOLDEN, "sphere_first_packets.npz"))
+    ref = fix["records"]
+    n = len(ref)
+    sim = octmps.read_deck(opt, mci)
+    mesh = octmps.build_mesh(mesh_path)
+    root = int(fix["root"])
+    assert mesh.find_root(float(fix["probe_x"])) == root
+    mult = octmps.safeprimes(3 + 3 * n)
+    rng = octmps.rng_init(mult, n, int(fix["seed"]))
+    p = oracle_py.params_from_sim(sim)
+    _, rec = oracle.run(p, mesh, (float(fix["probe_x"]), 0, 0), root, n, n, rng, 2, record=True)
+    return ref, rec
+
+
+def test_fp64_first_packets_match_reference(oracle, octmps):
+    """Event sequences (tet visited and event kind per step, generator states
+    at the end, detections, restores) of the first packet of 2000 lanes:
+    the FP64 restatement against the reference routine itself.  The
+    reference's log/sincos/acos are glibc's, the oracle's are its own, so a
+    last-bit difference in a direction can flip a discrete decision (most
+    often an exit through a matched-index face whose Fresnel R is exactly 0
+    in one and ~1e-32 in the other); the fraction of identical packets is
+    pinned from below."""
+    ref, rec = first_packet_match(oracle, octmps)
+    same = ((rec["hash"] == ref["hash"]) & (rec["x"] == ref["x"]) & (rec["xR"] == ref["xR"]) &
+            (rec["xS"] == ref["xS"]) & (rec["steps"] == ref["steps"]) &
+            (rec["detections"] == ref["detections"]) & (rec["restores"] == ref["restores"]))
+    assert same.mean() >= 0.90, same.mean()
+    c_ref, c_orc = ref["contribution"][same], rec["contribution"][same]
+    nz = c_ref != 0
+    assert np.all(np.abs(c_orc[nz] - c_ref[nz]) <= 1e-9 * np.abs(c_ref[nz]))
+    assert np.array_equal(c_orc[~nz], c_ref[~nz])
+
+
+def small_params(octmps, small_deck):
+    return oracle_py.params_from_sim(small_deck["sim"])
+
+
+@pytest.mark.parametrize("precision", [2, 0, 1])
+def test_oracle_tallies_within_3_sigma_of_reference(oracle, octmps, small_deck, precision):
+    """Full A-scans (20000 packets each) of the small mismatched-index deck:
+    the oracle with seeds independent of the reference runs, per-bin Class I
+    and Class II means compared within 3 combined standard errors."""
+    ref = np.load(os.path.join(GOLDEN, "small_ref_tallies.npz"))
+    sim = small_deck["sim"]
+    n = sim.number_of_photons
+    nb = sim.num_optical_depth_length_steps
+    runs = 4
+    ref_sum = {k: sum(ref[f"run{r}_{k}"] for r in range(runs)) for k in
+               ("sum1", "sumsq1", "sum2", "sumsq2", "count1", "count2")}
+    lanes = 2400
+    mult = octmps.safeprimes(3 + 3 * lanes)
+    p = small_params(octmps, small_deck)
+    acc = None
+    for seed in (11, 12, 13, 14):
+        rng = octmps.rng_init(mult, lanes, seed)
+        t = oracle.run(p, small_deck["mesh"], (sim.start_x, 0, 0), small_deck["root"], n, lanes,
+                       rng, precision)
+        assert t["packets"] == n and t["capped"] == 0
+        acc = t if acc is None else {k: acc[k] + t[k] for k in acc}
+    N = n * runs
+    for c in ("1", "2"):
+        frac, worst = three_sigma_ok(acc["sum" + c][:nb], acc["sumsq" + c][:nb], N,
+                                     ref_sum["sum" + c][:nb], ref_sum["sumsq" + c][:nb], N)
+        assert frac >= 0.98 and worst < 6.0, (c, frac, worst)
+    # detections per packet agree within 3 sigma (Poisson)
+    d_o = acc["num_filtered"]
+    d_r = sum(int(ref[f"run{r}_num_filtered"]) for r in range(runs))
+    assert abs(d_o - d_r) <= 3 * np.sqrt(d_o + d_r) + 1
+
+
+def test_oracle_is_deterministic(oracle, octmps, small_deck):
+    sim = small_deck["sim"]
+    lanes = 500
+    rng = octmps.rng_init(octmps.safeprimes(3 + 3 * lanes), lanes, 7)
+    p = small_params(octmps, small_deck)
+    a = oracle.run(p, small_deck["mesh"], (sim.start_x, 0, 0), small_deck["root"], 2000, lanes,
+                   rng, 0, n_threads=3)
+    b = oracle.run(p, small_deck["mesh"], (sim.start_x, 0, 0), small_deck["root"], 2000, lanes,
+                   rng, 0, n_threads=3)
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k])
