@@ -187,6 +187,9 @@ typedef struct {
     int32_t default_lanes;    /* RNG lanes per job when job.n_lanes = 0 */
     int32_t use_graphs;       /* replay launches through a CUDA graph */
     uint64_t hbm_budget_bytes;/* admission budget for job state; 0 = 80% of free */
+    int32_t scatter_share;    /* a warp runs its lanes' scattering step halves once at
+                                 least scatter_share/32 of its live lanes wait for one
+                                 (1..32; 0 = 10) */
 } octmps_launch_config;
 octmps_status octmps_ctx_configure(octmps_ctx *ctx, const octmps_launch_config *cfg);
 

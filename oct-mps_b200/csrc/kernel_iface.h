@@ -90,6 +90,8 @@ struct LaunchArgs {
     unsigned long long *next_unit;  // work counter, zeroed before the launch
     unsigned int *error;            // error word, zeroed before the launch
     uint64_t step_cap;              // steps allowed per packet
+    int32_t scatter_share;          // a warp runs the scattering halves of its steps once
+                                    // at least scatter_share/32 of its live lanes wait
 };
 
 // Error bits reported through LaunchArgs::error.

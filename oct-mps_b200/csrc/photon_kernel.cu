@@ -31,6 +31,11 @@ namespace {
 
 constexpr int kBlock = 256;
 
+// Outcomes of the first half of a step.
+constexpr int kDone = 0;     // step finished, packet continues
+constexpr int kEnd = 1;      // step finished, packet ended
+constexpr int kPending = 2;  // no face reached: scattering still to do
+
 template <typename T>
 struct Plane4;
 template <>
@@ -340,9 +345,12 @@ struct Lane {
         }
     }
 
-    // One propagation step: OCTMPSKernel's loop body
-    // (src/octmps_kernel.cuh:1351-1392).  Returns true when the packet ends.
-    __device__ __forceinline__ bool step(SplitCopy<T, P> &cont, unsigned int *err) {
+    // First half of a propagation step, OCTMPSKernel's loop body
+    // (src/octmps_kernel.cuh:1351-1392): step size, boundary test, hop and,
+    // when a face is reached, reflection or transmission and the roulette.
+    // Returns kDone, kEnd (the packet ended) or kPending (no face reached:
+    // the step continues in phase_b).
+    __device__ __forceinline__ int phase_a(SplitCopy<T, P> &cont, unsigned int *err) {
         int ev = 0;
         // ComputeStepSize, :505-515
         if (sleft == (T)0) {
@@ -389,7 +397,7 @@ struct Lane {
         if (hit) {
             if (face < 0) {
                 atomicOr(err, kErrNoExitFace);
-                return true;
+                return kEnd;
             }
             // FastReflectTransmit, :590-775
             if (kRecord) ++rhits;
@@ -465,17 +473,29 @@ struct Lane {
                 ev = 3;
             }
         } else {
-            ev = 1;
-            if (kRecord) ++rscatters;
-            // Drop, :584-588
-            w = DevNum<T>::mad(-w, rg.mua_muas, w);
-            if (type_bias == 0) {
-                rotate(spin_theta(rg.g), ux, uy, uz, false);
-            } else if (type_bias == 37) {
-                spin_bias(cont);
-            }
+            return kPending;  // the scattering half of the step runs in phase_b
         }
-        // Roulette, :1376-1392
+        return finish(ev, cont) ? kEnd : kDone;
+    }
+
+    // Second half of a step that did not reach a face: Drop, then Spin or
+    // SpinBias (:1359-1369), then the roulette.  Returns true when the
+    // packet ends.
+    __device__ __forceinline__ bool phase_b(SplitCopy<T, P> &cont) {
+        if (kRecord) ++rscatters;
+        // Drop, :584-588
+        w = DevNum<T>::mad(-w, rg.mua_muas, w);
+        if (type_bias == 0) {
+            rotate(spin_theta(rg.g), ux, uy, uz, false);
+        } else if (type_bias == 37) {
+            spin_bias(cont);
+        }
+        return finish(1, cont);
+    }
+
+    // Roulette, :1376-1392, and the step's record.  Returns true when the
+    // packet ends.
+    __device__ __forceinline__ bool finish(int ev, SplitCopy<T, P> &cont) {
         bool end = false;
         if (w < DevNum<T>::weight) {
             const T rnd = rand_co_G();
@@ -533,7 +553,22 @@ __global__ void __launch_bounds__(kBlock)
     uint64_t record_lane = ~0ull;  // lane whose first packet is being recorded
     bool recording = false;
 
+    // Lanes of this warp still in the loop, and whether this lane's current
+    // step waits for its scattering half.  A warp runs, per iteration, either
+    // the first half of a step on its lanes that have one to start, or the
+    // scattering half on the lanes waiting for it; it switches to the
+    // scattering half once at least kScatterShare/32 of its live lanes wait
+    // (or no lane can start a step).  Each lane still performs exactly the
+    // reference's sequence of operations; only the interleaving of lanes
+    // changes, so the warp executes the long scattering code for many lanes
+    // at once instead of on almost every iteration.
+    unsigned live = 0xffffffffu;
+    bool pending = false;
+    const int share = args.scatter_share;
+
     for (;;) {
+        bool has_work = true;
+        bool idle = false;
         if (packets_left == 0) {
             if (L.jd) {
                 atomicAdd(&L.jd->stats[0], (unsigned long long)steps_unit);
@@ -544,41 +579,69 @@ __global__ void __launch_bounds__(kBlock)
             steps_unit = packets_unit = capped = 0;
             L.restores_ = 0;
             const unsigned long long u = atomicAdd(args.next_unit, 1ull);
-            if (u >= args.total_units) break;
-            int lo = 0, hi = args.n_jobs - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (__ldg(args.unit_base + mid) <= u) lo = mid;
-                else hi = mid - 1;
+            if (u >= args.total_units) {
+                has_work = false;
+            } else {
+                int lo = 0, hi = args.n_jobs - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (__ldg(args.unit_base + mid) <= u) lo = mid;
+                    else hi = mid - 1;
+                }
+                const JobDesc *jd = args.jobs + lo;
+                const uint64_t v = u - __ldg(args.unit_base + lo);
+                if (jd != L.jd) {
+                    L.jd = jd;
+                    L.regions = reinterpret_cast<const RegionConst<T> *>(jd->regions);
+                    L.planes = jd->planes;
+                    L.adj = reinterpret_cast<const int4 *>(jd->adj);
+                    L.px = (T)jd->probe_x;
+                    L.py = (T)jd->probe_y;
+                    L.pz = (T)jd->probe_z;
+                    L.type_bias = jd->type_bias;
+                    L.region = -1;
+                }
+                L.xG = jd->rng_x[v];
+                L.aG = jd->rng_a[v];
+                L.xR = jd->rng_xR[v];
+                L.aR = jd->rng_aR[v];
+                L.xS = jd->rng_xS[v];
+                L.aS = jd->rng_aS[v];
+                const uint64_t nl = jd->n_lanes;
+                packets_left = jd->n_photons / nl + (v < jd->n_photons % nl ? 1 : 0);
+                if (packets_left == 0) {
+                    idle = true;  // a lane without packets: take another unit next time
+                } else {
+                    L.launch();
+                    steps_packet = 0;
+                    pending = false;
+                    recording = kRecord && records && lo == 0;
+                    record_lane = v;
+                }
             }
-            const JobDesc *jd = args.jobs + lo;
-            const uint64_t v = u - __ldg(args.unit_base + lo);
-            if (jd != L.jd) {
-                L.jd = jd;
-                L.regions = reinterpret_cast<const RegionConst<T> *>(jd->regions);
-                L.planes = jd->planes;
-                L.adj = reinterpret_cast<const int4 *>(jd->adj);
-                L.px = (T)jd->probe_x;
-                L.py = (T)jd->probe_y;
-                L.pz = (T)jd->probe_z;
-                L.type_bias = jd->type_bias;
-                L.region = -1;
-            }
-            L.xG = jd->rng_x[v];
-            L.aG = jd->rng_a[v];
-            L.xR = jd->rng_xR[v];
-            L.aR = jd->rng_aR[v];
-            L.xS = jd->rng_xS[v];
-            L.aS = jd->rng_aS[v];
-            const uint64_t nl = jd->n_lanes;
-            packets_left = jd->n_photons / nl + (v < jd->n_photons % nl ? 1 : 0);
-            if (packets_left == 0) continue;
-            L.launch();
-            steps_packet = 0;
-            recording = kRecord && records && lo == 0;
-            record_lane = v;
         }
-        const bool end = L.step(cont, args.error);
+        // The two vote sites below are reached by every live lane in every
+        // iteration.
+        live = __ballot_sync(live, has_work);
+        if (!has_work) break;
+        const unsigned pend = __ballot_sync(live, pending && !idle);
+        const unsigned ready = __ballot_sync(live, !pending && !idle);
+        const bool run_b = ready == 0u || __popc(pend) * 32 >= share * __popc(live);
+        if (idle) continue;
+        bool end;
+        if (run_b) {
+            if (!pending) continue;
+            pending = false;
+            end = L.phase_b(cont);
+        } else {
+            if (pending) continue;
+            const int r = L.phase_a(cont, args.error);
+            if (r == kPending) {
+                pending = true;
+                continue;
+            }
+            end = r == kEnd;
+        }
         ++steps_packet;
         bool done = end;
         if (!done && steps_packet >= args.step_cap) {

@@ -218,6 +218,7 @@ octmps_status flush_locked(octmps_ctx *ctx) {
         // A packet needs ~10^2-10^4 steps; a photon caught in degenerate
         // geometry (stepping s = 0 around an edge) is stopped and flagged.
         a.step_cap = 1ull << 26;
+        a.scatter_share = ctx->cfg.scatter_share > 0 ? ctx->cfg.scatter_share : 10;
         int regs = 0, per_sm = 0;
         int st = photon_kernel_attributes(prec, 256, &regs, &per_sm);
         if (st) return cuda_fail(ctx, (cudaError_t)st, "kernel attributes");

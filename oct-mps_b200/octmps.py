@@ -112,6 +112,7 @@ class LaunchConfig(C.Structure):
     _fields_ = [
         ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("default_lanes", C.c_int32),
         ("use_graphs", C.c_int32), ("hbm_budget_bytes", C.c_uint64),
+        ("scatter_share", C.c_int32),
     ]
 
 
@@ -351,8 +352,8 @@ class Context:
         a = np.ascontiguousarray(a, dtype=np.uint32)
         _check(lib().octmps_ctx_set_multipliers(self.h, _ptr(a, C.c_uint32), len(a)), self.h)
 
-    def configure(self, blocks_per_sm=0, default_lanes=0, hbm_budget_bytes=0):
-        cfg = LaunchConfig(0, blocks_per_sm, default_lanes, 0, hbm_budget_bytes)
+    def configure(self, blocks_per_sm=0, default_lanes=0, hbm_budget_bytes=0, scatter_share=0):
+        cfg = LaunchConfig(0, blocks_per_sm, default_lanes, 0, hbm_budget_bytes, scatter_share)
         _check(lib().octmps_ctx_configure(self.h, C.byref(cfg)), self.h)
 
     def upload_mesh(self, mesh):

@@ -50,7 +50,7 @@ def workdir(tmp_path_factory):
 @pytest.fixture(scope="session")
 def multipliers(octmps):
     """The generated multiplier table (the reference's safe-prime list is not shipped)."""
-    return octmps.safeprimes(3 + 3 * 30000)
+    return octmps.safeprimes(3 + 3 * 88800)  # enough for the default 88,800 lanes
 
 
 @pytest.fixture(scope="session")

@@ -20,6 +20,10 @@ pytestmark = pytest.mark.gpu
 
 REC_BYTES = oracle_py.PACKET_DTYPE.itemsize
 SUM_RTOL = {0: 1e-12, 1: 1e-5, 2: 1e-12}
+# The all-FP32 form accumulates with float atomics, which flush subnormal
+# results to zero (squares of contributions below ~1e-19 vanish on the
+# device, not in the oracle).
+SUM_ATOL = {0: 0.0, 1: 1e-37, 2: 0.0}
 
 
 @pytest.fixture(scope="module")
@@ -68,7 +72,7 @@ def assert_tallies_equal(t_gpu, t_orc, precision, nbins):
         np.testing.assert_array_equal(t_gpu[k], t_orc[k], err_msg=k)
     for k in ("sum1", "sumsq1", "sum2", "sumsq2"):
         np.testing.assert_allclose(t_gpu[k][:nbins], t_orc[k][:nbins], rtol=SUM_RTOL[precision],
-                                   atol=0, err_msg=k)
+                                   atol=SUM_ATOL[precision], err_msg=k)
     for k in ("max1", "max2"):
         np.testing.assert_array_equal(t_gpu[k][:nbins], t_orc[k][:nbins], err_msg=k)
 
