@@ -171,7 +171,7 @@ struct Lane {
     }
 
     // Class I/II tally, src/octmps_kernel.cuh:684-744.
-    __device__ void tally(T r_fresnel) {
+    __device__ __noinline__ void tally(T r_fresnel) {
         const JobDesc &J = *jd;
         const TallyLayout L = tally_layout(J.nbins, sizeof(P));
         unsigned char *base = reinterpret_cast<unsigned char *>(J.tally);
@@ -540,8 +540,10 @@ struct Lane {
     uint32_t restores_;
 };
 
-template <typename T, typename P, bool kRecord>
-__global__ void __launch_bounds__(kBlock)
+// kMinBlocks: resident blocks per SM the register allocation must allow
+// (2: up to 128 registers per thread; 3: up to 80).
+template <typename T, typename P, bool kRecord, int kMinBlocks>
+__global__ void __launch_bounds__(kBlock, kMinBlocks)
     photon_kernel(const LaunchArgs args, PacketRecordDev *records) {
     __shared__ SplitCopy<T, P> cont_all[kBlock];
     SplitCopy<T, P> &cont = cont_all[threadIdx.x];
@@ -680,38 +682,45 @@ __global__ void __launch_bounds__(kBlock)
 
 }  // namespace
 
-int launch_photon_kernel(int precision, const LaunchArgs &args, int grid, int block, void *stream,
-                         void *records) {
+namespace {
+
+template <typename T, typename P>
+const void *pick(int min_blocks, bool record) {
+    if (record) return (const void *)photon_kernel<T, P, true, 2>;
+    switch (min_blocks) {
+        case 2: return (const void *)photon_kernel<T, P, false, 2>;
+        case 3: return (const void *)photon_kernel<T, P, false, 3>;
+        default: return nullptr;
+    }
+}
+
+const void *photon_kernel_fn(int precision, int min_blocks, bool record) {
+    switch (precision) {
+        case kMixed: return pick<float, double>(min_blocks, record);
+        case kFP32: return pick<float, float>(min_blocks, record);
+        case kFP64: return pick<double, double>(min_blocks == 3 ? 2 : min_blocks, record);
+        default: return nullptr;
+    }
+}
+
+}  // namespace
+
+int launch_photon_kernel(int precision, int min_blocks, const LaunchArgs &args, int grid,
+                         int block, void *stream, void *records) {
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     PacketRecordDev *rec = reinterpret_cast<PacketRecordDev *>(records);
     if (block != kBlock) return (int)cudaErrorInvalidValue;
-    if (rec) {
-        switch (precision) {
-            case kMixed: photon_kernel<float, double, true><<<grid, block, 0, st>>>(args, rec); break;
-            case kFP32: photon_kernel<float, float, true><<<grid, block, 0, st>>>(args, rec); break;
-            case kFP64: photon_kernel<double, double, true><<<grid, block, 0, st>>>(args, rec); break;
-            default: return (int)cudaErrorInvalidValue;
-        }
-    } else {
-        switch (precision) {
-            case kMixed: photon_kernel<float, double, false><<<grid, block, 0, st>>>(args, nullptr); break;
-            case kFP32: photon_kernel<float, float, false><<<grid, block, 0, st>>>(args, nullptr); break;
-            case kFP64: photon_kernel<double, double, false><<<grid, block, 0, st>>>(args, nullptr); break;
-            default: return (int)cudaErrorInvalidValue;
-        }
-    }
-    return (int)cudaGetLastError();
+    const void *fn = photon_kernel_fn(precision, min_blocks, rec != nullptr);
+    if (!fn) return (int)cudaErrorInvalidValue;
+    void *params[2] = {const_cast<LaunchArgs *>(&args), &rec};
+    return (int)cudaLaunchKernel(fn, dim3(grid), dim3(block), params, 0, st);
 }
 
-int photon_kernel_attributes(int precision, int block, int *regs, int *max_blocks_per_sm) {
+int photon_kernel_attributes(int precision, int block, int min_blocks, int *regs,
+                             int *max_blocks_per_sm) {
     cudaFuncAttributes a;
-    const void *fn = nullptr;
-    switch (precision) {
-        case kMixed: fn = (const void *)photon_kernel<float, double, false>; break;
-        case kFP32: fn = (const void *)photon_kernel<float, float, false>; break;
-        case kFP64: fn = (const void *)photon_kernel<double, double, false>; break;
-        default: return (int)cudaErrorInvalidValue;
-    }
+    const void *fn = photon_kernel_fn(precision, min_blocks, false);
+    if (!fn) return (int)cudaErrorInvalidValue;
     cudaError_t e = cudaFuncGetAttributes(&a, fn);
     if (e != cudaSuccess) return (int)e;
     *regs = a.numRegs;

@@ -30,6 +30,13 @@ using namespace octmps;
 
 namespace {
 
+// Resident blocks per SM the default kernel variant is compiled for, and the
+// share of a warp's live lanes (in 32nds) that must wait for the scattering
+// half of their step before the warp runs it; both the best of a sweep on
+// the B-scan workload (2 blocks: 128-register cap, no spills).
+constexpr int kDefaultMinBlocks = 2;
+constexpr int kDefaultScatterShare = 16;
+
 double now_ms() {
     return std::chrono::duration<double, std::milli>(
                std::chrono::steady_clock::now().time_since_epoch())
@@ -218,11 +225,16 @@ octmps_status flush_locked(octmps_ctx *ctx) {
         // A packet needs ~10^2-10^4 steps; a photon caught in degenerate
         // geometry (stepping s = 0 around an edge) is stopped and flagged.
         a.step_cap = 1ull << 26;
-        a.scatter_share = ctx->cfg.scatter_share > 0 ? ctx->cfg.scatter_share : 10;
+        a.scatter_share = ctx->cfg.scatter_share > 0 ? ctx->cfg.scatter_share : kDefaultScatterShare;
+        // Variant compiled for 2 or 3 resident blocks per SM (register cap
+        // 128 or 80); the FP64 form has only the first.
+        int min_blocks = ctx->cfg.blocks_per_sm == 2 || ctx->cfg.blocks_per_sm == 3
+                             ? ctx->cfg.blocks_per_sm
+                             : kDefaultMinBlocks;
+        if (prec == kFP64 || ctx->record_buf) min_blocks = 2;
         int regs = 0, per_sm = 0;
-        int st = photon_kernel_attributes(prec, 256, &regs, &per_sm);
+        int st = photon_kernel_attributes(prec, 256, min_blocks, &regs, &per_sm);
         if (st) return cuda_fail(ctx, (cudaError_t)st, "kernel attributes");
-        if (ctx->cfg.blocks_per_sm > 0) per_sm = std::min(per_sm, (int)ctx->cfg.blocks_per_sm);
         if (per_sm < 1) per_sm = 1;
         const uint64_t max_useful = (units + 255) / 256;
         int grid = ctx->n_sm * per_sm;
@@ -230,7 +242,7 @@ octmps_status flush_locked(octmps_ctx *ctx) {
         CK(cudaEventCreate(&L->start), "event");
         CK(cudaEventCreate(&L->stop), "event");
         CK(cudaEventRecord(L->start, ctx->stream), "event");
-        st = launch_photon_kernel(prec, a, grid, 256, ctx->stream, ctx->record_buf);
+        st = launch_photon_kernel(prec, min_blocks, a, grid, 256, ctx->stream, ctx->record_buf);
         if (st) return cuda_fail(ctx, (cudaError_t)st, "photon kernel launch");
         CK(cudaMemcpyAsync(L->error_host, a.error, sizeof(unsigned int), cudaMemcpyDeviceToHost,
                            ctx->stream),
