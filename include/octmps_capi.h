@@ -189,7 +189,7 @@ typedef struct {
     uint64_t hbm_budget_bytes;/* admission budget for job state; 0 = 80% of free */
     int32_t scatter_share;    /* a warp runs its lanes' scattering step halves once at
                                  least scatter_share/32 of its live lanes wait for one
-                                 (1..32; 0 = 10) */
+                                 (1..32; 0 = 16) */
 } octmps_launch_config;
 octmps_status octmps_ctx_configure(octmps_ctx *ctx, const octmps_launch_config *cfg);
 
@@ -227,6 +227,66 @@ octmps_status octmps_read_mci(const char *path, octmps_sim *inout);
  * and FilteredPhotons.mco, in directory `dir` ("" = current). */
 octmps_status octmps_write_result(const char *dir, const octmps_sim *sim, double probe_x,
                                   const octmps_tally *t);
+
+/* ---- one A-scan without any allocation ----------------------------------------
+ * No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory, for instance an application that gives the
+ * library a fixed device arena and forbids further cudaMalloc (real-time or
+ * certified pipelines, or a host framework whose caching allocator owns all
+ * of device memory), or code running where an allocation could stall.
+ *
+ * octmps_ascan_run_noalloc runs one A-scan (mixed precision) through the same
+ * photon kernel as octmps_job_submit.  The caller passes every input and
+ * output in device memory it owns; the call allocates nothing (no cudaMalloc,
+ * cudaFree or allocating library routine).  What the kernel needs beyond the
+ * inputs and outputs (job descriptor, work counter, error word, statistics,
+ * region constants: OCTMPS_NOALLOC_SCRATCH_BYTES) lives in one fixed
+ * file-scope device array that every GPU loading the library holds until the
+ * process exits.  The first call on a device looks up that array's device
+ * address (once per device); make that first call before any stream capture.
+ * All calls on a device share the array, so calls whose work overlaps on the
+ * GPU race: serialise them.  The call returns after the A-scan finished.
+ *
+ * Device layouts the caller provides:
+ *   planes : float, 16 per tet: for face k = 0..3 the reference's face plane
+ *            (Nx, Ny, Nz, d) of tet_faces[k] times tet_signs[k]
+ *   adj    : int32, 4 per tet (16-byte aligned): -1 for a boundary face, else
+ *            neighbour | region_of_neighbour << 24 (meshes below 2^24 tets)
+ *   rng_*  : the lanes' generator states as octmps_rng_init fills them
+ *   tally  : OCTMPS_NOALLOC_TALLY_BYTES(nbins) bytes, zeroed by the call:
+ *            uint64 totals[4] (filtered, class I, class II, 0) at byte 0, then
+ *            uint64 count1[nbins+1], count2[nbins+1], then double sum1, sumsq1,
+ *            sum2, sumsq2, max1, max2 [nbins+2] each; every array starts on a
+ *            16-byte boundary.
+ * Errors: OCTMPS_ERR_INVALID_ARG for null pointers, more than
+ * OCTMPS_NOALLOC_MAX_REGIONS regions, glass regions (mus = 0), n_lanes 0 or
+ * above n_photons, root or tet counts out of range; OCTMPS_ERR_KERNEL if the
+ * kernel flagged a photon; OCTMPS_ERR_DEVICE on a CUDA error. */
+#define OCTMPS_NOALLOC_MAX_REGIONS 100
+#define OCTMPS_NOALLOC_SCRATCH_BYTES 2640 /* per GPU, held until exit */
+#define OCTMPS_NOALLOC_ROUND16(n) ((((uint64_t)(n)) + 15u) & ~(uint64_t)15u)
+#define OCTMPS_NOALLOC_TALLY_BYTES(nbins) \
+    (32u + 2u * OCTMPS_NOALLOC_ROUND16(((uint64_t)(nbins) + 1u) * 8u) + \
+     6u * OCTMPS_NOALLOC_ROUND16(((uint64_t)(nbins) + 2u) * 8u))
+typedef struct {
+    const octmps_sim *sim;          /* host memory; copied by the call */
+    const float *planes;            /* device */
+    const int32_t *adj;             /* device */
+    int32_t n_tets;
+    int32_t root_tet;               /* octmps_mesh_find_root */
+    int32_t root_region;            /* region of root_tet */
+    double probe_x, probe_y, probe_z;
+    uint64_t n_photons;
+    uint32_t n_lanes;               /* 1 .. n_photons */
+    const uint64_t *rng_x;          /* device, n_lanes each */
+    const uint32_t *rng_a;
+    const uint64_t *rng_xR;
+    const uint32_t *rng_aR;
+    const uint64_t *rng_xS;
+    const uint32_t *rng_aS;
+    void *tally;                    /* device */
+} octmps_noalloc_ascan;
+octmps_status octmps_ascan_run_noalloc(const octmps_noalloc_ascan *a, void *stream);
 
 /* ---- multiplier table generation (safeprimes_base32.txt) ---------------- */
 int octmps_safeprimes_generate(uint32_t *out, uint64_t count);

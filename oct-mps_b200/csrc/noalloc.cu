@@ -1,0 +1,186 @@
+// A-scan entry point that allocates no memory.
+//
+// Some callers of this library cannot call cudaMalloc: an application that
+// hands the library a fixed device arena at start-up and forbids any other
+// allocation (real-time or certified pipelines, or a host framework whose own
+// caching allocator owns all of device memory), or a caller running inside a
+// section where a device allocation could stall behind other work.  For them
+// this file runs one A-scan through the same photon kernel as
+// octmps_job_submit, with everything the kernel needs beyond the caller's
+// inputs and outputs (job descriptor, work-unit table, work counter, error
+// word, statistics, region constants) placed in one file-scope device array
+// of fixed size instead of in allocated memory.
+//
+// That array exists once per GPU that loads the library and stays allocated
+// until the process exits.  Every call on a device shares it and it keeps
+// the previous call's contents; the call rewrites all of it before the launch.
+// Two calls whose work overlaps on the GPU (different streams, or calls from
+// several host threads) race on it: serialise them.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cfloat>
+#include <cstring>
+#include <mutex>
+
+#include "kernel_iface.h"
+#include "octmps_host.h"
+
+using namespace octmps;
+
+namespace {
+
+// Scratch layout inside the array (offsets in bytes).
+constexpr size_t kJobOff = 0;                                        // JobDesc
+constexpr size_t kUnitOff = 512;                                     // uint64 unit_base[2]
+constexpr size_t kCounterOff = 544;                                  // work counter (u64)
+constexpr size_t kErrorOff = 552;                                    // error word (u32)
+constexpr size_t kStatsOff = 576;                                    // u64 stats[4]
+constexpr size_t kRegionOff = 640;                                   // RegionConst<float>[...]
+constexpr size_t kScratchBytes = kRegionOff + OCTMPS_NOALLOC_MAX_REGIONS * sizeof(RegionConst<float>);
+
+static_assert(sizeof(JobDesc) <= kUnitOff - kJobOff, "job descriptor does not fit its slot");
+static_assert(kScratchBytes == OCTMPS_NOALLOC_SCRATCH_BYTES, "scratch size differs from the header");
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+unsigned char *g_scratch_addr[kMaxDevices] = {nullptr};
+
+// Device address of the scratch array on the current device (looked up once
+// per device; the host-side symbol is not a device address).
+cudaError_t scratch_address(int device, unsigned char **out) {
+    std::lock_guard<std::mutex> g(g_mu);
+    if (!g_scratch_addr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_scratch_addr[device] = static_cast<unsigned char *>(p);
+    }
+    *out = g_scratch_addr[device];
+    return cudaSuccess;
+}
+
+double div_rd_host(double a, double b) {
+    double q = a / b;
+    if (!std::isfinite(q) || q == 0.0) return q;
+    double r = std::fma(-q, b, a);
+    if (r != 0.0 && ((r < 0.0) == (b > 0.0))) q = std::nextafter(q, -INFINITY);
+    return q;
+}
+
+}  // namespace
+
+static_assert(OCTMPS_NOALLOC_TALLY_BYTES(600) == 32 + 2 * 4816 + 6 * 4816,
+              "tally size formula");
+
+extern "C" octmps_status octmps_ascan_run_noalloc(const octmps_noalloc_ascan *a, void *stream) {
+    if (!a || !a->sim || !a->planes || !a->adj || !a->rng_x || !a->rng_a || !a->rng_xR ||
+        !a->rng_aR || !a->rng_xS || !a->rng_aS || !a->tally)
+        return OCTMPS_ERR_INVALID_ARG;
+    const octmps_sim &s = *a->sim;
+    if (s.n_regions < 2 || s.n_regions > OCTMPS_NOALLOC_MAX_REGIONS)
+        return OCTMPS_ERR_INVALID_ARG;  // the region table must fit the fixed scratch
+    if (a->n_tets < 1 || a->n_tets >= kMaxTetsPacked || a->root_tet < 0 ||
+        a->root_tet >= a->n_tets || a->root_region < 1 || a->root_region >= s.n_regions ||
+        a->n_lanes == 0 || a->n_photons < a->n_lanes || s.num_optical_depth_length_steps < 1)
+        return OCTMPS_ERR_INVALID_ARG;
+    for (int i = 1; i < s.n_regions; ++i)
+        if (s.regions[i].mus == 0.0) return OCTMPS_ERR_INVALID_ARG;  // glass needs FP64
+
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices)
+        return OCTMPS_ERR_NO_DEVICE;
+    unsigned char *scratch = nullptr;
+    if (scratch_address(device, &scratch) != cudaSuccess) return OCTMPS_ERR_DEVICE;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+
+    // Host image of the scratch area (stack memory; no allocation).
+    unsigned char img[kScratchBytes];
+    memset(img, 0, sizeof img);
+    RegionConst<float> *rg = reinterpret_cast<RegionConst<float> *>(img + kRegionOff);
+    for (int i = 0; i < s.n_regions; ++i) {
+        // read_simulation_data (src/octmps_io.cpp:625-626) and
+        // InitDeviceConstantMemory (src/octmps_kernel.cuh:204-214).
+        const double mutr = 1.0 / (s.regions[i].mua + s.regions[i].mus);
+        rg[i].n = (float)s.regions[i].n;
+        rg[i].muas = (float)(1.0 / mutr);
+        rg[i].rmuas = (float)mutr;
+        rg[i].mua_muas = (float)(s.regions[i].mua * mutr);
+        rg[i].g = (float)s.regions[i].g;
+    }
+    JobDesc D;
+    memset(&D, 0, sizeof D);
+    D.planes = a->planes;
+    D.adj = a->adj;
+    D.regions = scratch + kRegionOff;
+    D.rng_x = const_cast<uint64_t *>(a->rng_x);
+    D.rng_a = const_cast<uint32_t *>(a->rng_a);
+    D.rng_xR = const_cast<uint64_t *>(a->rng_xR);
+    D.rng_aR = const_cast<uint32_t *>(a->rng_aR);
+    D.rng_xS = const_cast<uint64_t *>(a->rng_xS);
+    D.rng_aS = const_cast<uint32_t *>(a->rng_aS);
+    D.tally = a->tally;
+    D.stats = reinterpret_cast<unsigned long long *>(scratch + kStatsOff);
+    D.n_photons = a->n_photons;
+    D.n_lanes = a->n_lanes;
+    D.n_tets = a->n_tets;
+    D.probe_x = a->probe_x;
+    D.probe_y = a->probe_y;
+    D.probe_z = a->probe_z;
+    const double n0 = s.regions[0].n, nr = s.regions[a->root_region].n;
+    const double rs = (n0 - nr) / (n0 + nr);  // Rspecular, src/main.cu:29-37
+    D.w0 = 1.0 - rs * rs;
+    D.tdmin = s.target_depth_min;
+    D.tdmax = s.target_depth_max;
+    D.bias_a = s.backward_bias_coefficient;
+    D.p_bias = s.probability_additional_bias;
+    D.cos_collect = cos(s.max_collecting_angle_deg * 3.14159265359 / 180.0);
+    D.radius = s.max_collecting_radius;
+    D.rnd_step = s.rnd_step_size_in_tissue;
+    D.n_ambient = s.regions[0].n;
+    D.shift = s.optical_depth_shift;
+    D.bin_width = div_rd_host(s.coherence_length_source, 6.0);
+    D.half_lc = div_rd_host(s.coherence_length_source, 2.0);
+    D.root_tet = a->root_tet;
+    D.root_region = a->root_region;
+    D.type_bias = s.type_bias;
+    D.nbins = s.num_optical_depth_length_steps;
+    memcpy(img + kJobOff, &D, sizeof D);
+    uint64_t *ub = reinterpret_cast<uint64_t *>(img + kUnitOff);
+    ub[0] = 0;
+    ub[1] = a->n_lanes;
+    // counter, error word and statistics start at zero (img is zeroed)
+
+    if (cudaMemcpyAsync(scratch, img, sizeof img, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return OCTMPS_ERR_DEVICE;
+    if (tally_layout(D.nbins, sizeof(double)).bytes != OCTMPS_NOALLOC_TALLY_BYTES(D.nbins))
+        return OCTMPS_ERR_INVALID_ARG;
+    if (cudaMemsetAsync(a->tally, 0, OCTMPS_NOALLOC_TALLY_BYTES(D.nbins), st) != cudaSuccess)
+        return OCTMPS_ERR_DEVICE;
+    LaunchArgs L;
+    L.jobs = reinterpret_cast<const JobDesc *>(scratch + kJobOff);
+    L.unit_base = reinterpret_cast<const uint64_t *>(scratch + kUnitOff);
+    L.n_jobs = 1;
+    L.total_units = a->n_lanes;
+    L.next_unit = reinterpret_cast<unsigned long long *>(scratch + kCounterOff);
+    L.error = reinterpret_cast<unsigned int *>(scratch + kErrorOff);
+    L.step_cap = 1ull << 26;
+    L.scatter_share = 10;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        return OCTMPS_ERR_DEVICE;
+    int regs = 0, per_sm = 0;
+    if (photon_kernel_attributes(kMixed, 256, 2, &regs, &per_sm) != 0 || per_sm < 1) per_sm = 1;
+    uint64_t grid = (uint64_t)sms * per_sm;
+    const uint64_t useful = (a->n_lanes + 255) / 256;
+    if (grid > useful) grid = useful;
+    if (launch_photon_kernel(kMixed, 2, L, (int)grid, 256, st, nullptr) != 0)
+        return OCTMPS_ERR_DEVICE;
+    unsigned int err = 0;
+    if (cudaMemcpyAsync(&err, L.error, sizeof err, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return OCTMPS_ERR_DEVICE;
+    return err ? OCTMPS_ERR_KERNEL : OCTMPS_OK;
+}

@@ -124,7 +124,7 @@ EXPORTED = [
     "octmps_rng_init", "octmps_job_submit", "octmps_ctx_flush", "octmps_job_wait",
     "octmps_job_fetch", "octmps_job_fetch_stats", "octmps_job_release", "octmps_read_opt",
     "octmps_read_mci", "octmps_write_result", "octmps_safeprimes_generate",
-    "octmps_safeprimes_write", "octmps_safeprimes_read",
+    "octmps_safeprimes_write", "octmps_safeprimes_read", "octmps_ascan_run_noalloc",
 ]
 
 _lib = None
