@@ -248,10 +248,13 @@ struct Lane {
             uz = copysign_form ? copysignT(cost, az * cost) : cost * (az >= (T)0 ? (T)1 : (T)-1);
         } else {
             // RSQRT(x) taken as 1/sqrt(x), both correctly rounded.
-            const T temp = rcpT(sqrtT(DevNum<T>::mad(-az, az, (T)1)));
+            const T sq = sqrtT(DevNum<T>::mad(-az, az, (T)1));
+            const T temp = rcpT(sq);
             ux = DevNum<T>::mad(DevNum<T>::mad(stcp * ax, az, -(stsp * ay)), temp, ax * cost);
             uy = DevNum<T>::mad(DevNum<T>::mad(stcp * ay, az, stsp * ax), temp, ay * cost);
-            uz = DevNum<T>::mad(az, cost, DevNum<T>::div(-stcp, temp));
+            // FAST_DIV(-stcp, temp) = -stcp * sqrt(1 - uz^2): multiplied in
+            // the FP32 forms, divided in the FP64 form
+            uz = DevNum<T>::mad(az, cost, kFused<T> ? -(stcp * sq) : DevNum<T>::div(-stcp, temp));
         }
     }
 
@@ -289,13 +292,23 @@ struct Lane {
         T vy = py - y;
         T vz = pz - z;
         const T len = sqrtT(DevNum<T>::mad(vz, vz, DevNum<T>::mad(vx, vx, vy * vy)));
-        vx = DevNum<T>::div(vx, len);
-        vy = DevNum<T>::div(vy, len);
-        vz = DevNum<T>::div(vz, len);
+        if (kFused<T>) {
+            const T rl = rcpT(len);  // FP32 forms: one reciprocal, three products
+            vx *= rl;
+            vy *= rl;
+            vz *= rl;
+        } else {
+            vx = DevNum<T>::div(vx, len);
+            vy = DevNum<T>::div(vy, len);
+            vz = DevNum<T>::div(vz, len);
+        }
         if ((fst_flag || num_back > 0) && !reached) {
             reached = 2;
-            const T next_step = DevNum<T>::div(-log_method((T)J.rnd_step), rg.muas);
-            if (next_step >= len && -vz >= (T)J.cos_collect) reached = 1;
+            // -log(0)/mu_t is +infinity: with rndStepSizeInTissue = 0 the
+            // distance test always holds.
+            const T rs = (T)J.rnd_step;
+            const bool far = rs == (T)0 || DevNum<T>::div(-log_method(rs), rg.muas) >= len;
+            if (far && -vz >= (T)J.cos_collect) reached = 1;
             btmp = (T)J.bias_a;
         }
         int sel = 0;
@@ -370,15 +383,39 @@ struct Lane {
         T min_d = DevNum<T>::big;
         T min_cos = 0;
         int face = -1;
+        if (kFused<T>) {
+            // FP32 forms: nearest face by perp_i * c_j < perp_j * c_i
+            // (c = -cos > 0), one division for the winner.
+            T best_perp = 0, best_c = 0;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (cosv[k] < (T)0) {
-                const T perp = dot3<T>(pl.v[k][0], pl.v[k][1], pl.v[k][2], x, y, z) + pl.v[k][3];
-                const T t = DevNum<T>::div(-perp, cosv[k]);
-                if (t < min_d) {
-                    min_d = t;
-                    face = k;
-                    min_cos = cosv[k];
+            for (int k = 0; k < 4; ++k) {
+                if (cosv[k] < (T)0) {
+                    const T perp = dot3<T>(pl.v[k][0], pl.v[k][1], pl.v[k][2], x, y, z) + pl.v[k][3];
+                    const T c = -cosv[k];
+                    const bool nearer = face < 0 ? perp < DevNum<T>::big * c
+                                                 : perp * best_c < best_perp * c;
+                    if (nearer) {
+                        best_perp = perp;
+                        best_c = c;
+                        face = k;
+                    }
+                }
+            }
+            if (face >= 0) {
+                min_d = DevNum<T>::div(best_perp, best_c);
+                min_cos = -best_c;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (cosv[k] < (T)0) {
+                    const T perp = dot3<T>(pl.v[k][0], pl.v[k][1], pl.v[k][2], x, y, z) + pl.v[k][3];
+                    const T t = DevNum<T>::div(-perp, cosv[k]);
+                    if (t < min_d) {
+                        min_d = t;
+                        face = k;
+                        min_cos = cosv[k];
+                    }
                 }
             }
         }
@@ -406,26 +443,33 @@ struct Lane {
             const int next_region = entry < 0 ? 0 : (int)((uint32_t)entry >> kAdjIndexBits);
             const T nt = entry < 0 ? (T)jd->n_ambient
                                    : __ldg(reinterpret_cast<const T *>(regions + next_region));
-            const T ni_nt = DevNum<T>::div(rg.n, nt);
+            T r;
             T sa1 = sqrtT(DevNum<T>::mad(-ca1, ca1, (T)1));
             if (ca1 > DevNum<T>::coszero) sa1 = 0;
-            const T sa2 = fminT(ni_nt * sa1, (T)1);
-            const T ca2 = sqrtT(DevNum<T>::mad(-sa2, sa2, (T)1));
-            const T ca1ca2 = ca1 * ca2;
-            const T sa1sa2 = sa1 * sa2;
-            T sa1ca2 = sa1 * ca2;
-            T ca1sa2 = ca1 * sa2;
-            if (ca1 > DevNum<T>::coszero) {
-                sa1ca2 = 1;
-                ca1sa2 = ni_nt;
+            if (kFused<T> && rg.n == nt) {
+                // FP32 forms, matched refractive indices: R is exactly 0
+                // except for the grazing-incidence rule (sa2 = sa1 here).
+                r = (ca1 < DevNum<T>::cos90 || sa1 == (T)1) ? (T)1 : (T)0;
+            } else {
+                const T ni_nt = DevNum<T>::div(rg.n, nt);
+                const T sa2 = fminT(ni_nt * sa1, (T)1);
+                const T ca2 = sqrtT(DevNum<T>::mad(-sa2, sa2, (T)1));
+                const T ca1ca2 = ca1 * ca2;
+                const T sa1sa2 = sa1 * sa2;
+                T sa1ca2 = sa1 * ca2;
+                T ca1sa2 = ca1 * sa2;
+                if (ca1 > DevNum<T>::coszero) {
+                    sa1ca2 = 1;
+                    ca1sa2 = ni_nt;
+                }
+                const T cam = ca1ca2 + sa1sa2;
+                const T sap = sa1ca2 + ca1sa2;
+                const T sam = sa1ca2 - ca1sa2;
+                r = DevNum<T>::div(sam, sap * cam);
+                r = r * r;
+                r = r * DevNum<T>::mad(ca1ca2, ca1ca2, sa1sa2 * sa1sa2);
+                if (ca1 < DevNum<T>::cos90 || sa2 == (T)1) r = 1;
             }
-            const T cam = ca1ca2 + sa1sa2;
-            const T sap = sa1ca2 + ca1sa2;
-            const T sam = sa1ca2 - ca1sa2;
-            T r = DevNum<T>::div(sam, sap * cam);
-            r = r * r;
-            r = r * DevNum<T>::mad(ca1ca2, ca1ca2, sa1sa2 * sa1sa2);
-            if (ca1 < DevNum<T>::cos90 || sa2 == (T)1) r = 1;
 
             const T fnx = face == 0 ? pl.v[0][0] : face == 1 ? pl.v[1][0] : face == 2 ? pl.v[2][0] : pl.v[3][0];
             const T fny = face == 0 ? pl.v[0][1] : face == 1 ? pl.v[1][1] : face == 2 ? pl.v[2][1] : pl.v[3][1];
@@ -551,7 +595,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     L.jd = nullptr;
     L.region = -1;
     L.restores_ = 0;
-    uint64_t packets_left = 0, steps_packet = 0, steps_unit = 0, packets_unit = 0, capped = 0;
+    // packets still to run in the current unit (the runtime keeps a job's
+    // packets per lane below 2^32) and steps of the current packet (capped
+    // at step_cap <= 2^32)
+    uint32_t packets_left = 0, steps_packet = 0;
     uint64_t record_lane = ~0ull;  // lane whose first packet is being recorded
     bool recording = false;
 
@@ -572,14 +619,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
         bool has_work = true;
         bool idle = false;
         if (packets_left == 0) {
-            if (L.jd) {
-                atomicAdd(&L.jd->stats[0], (unsigned long long)steps_unit);
-                atomicAdd(&L.jd->stats[1], (unsigned long long)L.restores_);
-                atomicAdd(&L.jd->stats[2], (unsigned long long)packets_unit);
-                if (capped) atomicAdd(&L.jd->stats[3], (unsigned long long)capped);
-            }
-            steps_unit = packets_unit = capped = 0;
-            L.restores_ = 0;
             const unsigned long long u = atomicAdd(args.next_unit, 1ull);
             if (u >= args.total_units) {
                 has_work = false;
@@ -610,7 +649,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
                 L.xS = jd->rng_xS[v];
                 L.aS = jd->rng_aS[v];
                 const uint64_t nl = jd->n_lanes;
-                packets_left = jd->n_photons / nl + (v < jd->n_photons % nl ? 1 : 0);
+                packets_left = (uint32_t)(jd->n_photons / nl + (v < jd->n_photons % nl ? 1 : 0));
                 if (packets_left == 0) {
                     idle = true;  // a lane without packets: take another unit next time
                 } else {
@@ -648,12 +687,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
         bool done = end;
         if (!done && steps_packet >= args.step_cap) {
             atomicOr(args.error, kErrStepCap);
-            ++capped;
+            atomicAdd(&L.jd->stats[3], 1ull);
             done = true;
         }
         if (done) {
-            steps_unit += steps_packet;
-            ++packets_unit;
+            // per-packet statistics: steps, split copies resumed, packets
+            atomicAdd(&L.jd->stats[0], (unsigned long long)steps_packet);
+            if (L.restores_) atomicAdd(&L.jd->stats[1], (unsigned long long)L.restores_);
+            atomicAdd(&L.jd->stats[2], 1ull);
+            L.restores_ = 0;
             if (kRecord && recording) {
                 PacketRecordDev r;
                 r.hash = L.rhash;

@@ -202,6 +202,12 @@ struct DevNum<double> {
     static constexpr double big = 1.0e10;
 };
 
+// The FP32 forms (fused multiply-adds) also take a few cheaper, equally
+// accurate formulations of the same quantities; the FP64 form keeps the
+// reference's operations.
+template <typename T>
+constexpr bool kFused = sizeof(T) == sizeof(float);
+
 // a.x + b.y + c.z as (a.x + b.y) + c.z, the reference's order.
 template <typename T>
 __device__ __forceinline__ T dot3(T a, T b, T c, T x, T y, T z) {

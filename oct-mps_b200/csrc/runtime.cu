@@ -471,6 +471,8 @@ octmps_status octmps_job_submit(octmps_ctx *ctx, const octmps_job *job, octmps_j
         lanes = (uint32_t)std::min<uint64_t>(n_ph, def);
     }
     if ((uint64_t)lanes > n_ph) lanes = (uint32_t)n_ph;
+    if (n_ph / lanes >= 0xffffffffull)
+        return fail(ctx, OCTMPS_ERR_INVALID_ARG, "more than 2^32 packets per RNG lane");
     if (ctx->multipliers.size() < 3 + 3 * (uint64_t)lanes)
         return fail(ctx, OCTMPS_ERR_INVALID_ARG, "multiplier table too short for the lane count");
     const uint64_t seed = job->seed ? job->seed : 985456376ull;

@@ -11,6 +11,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 namespace {
@@ -243,6 +244,12 @@ inline T rand_oc(uint64_t *x, uint32_t a) {
     return (T)1 - rand_co<T>(x, a);
 }
 
+// The FP32 forms (fused multiply-adds) also take a few cheaper but equally
+// accurate formulations of the same quantities; the FP64 form keeps the
+// reference's operations.
+template <typename T>
+constexpr bool kFused = std::is_same<T, float>::value;
+
 // a.x + b.y + c.z evaluated left to right, (a.x + b.y) + c.z, as the
 // reference writes its dot products; fused in the FP32 forms.
 template <typename T>
@@ -355,15 +362,40 @@ struct Lane {
         }
         T min_d = Num<T>::big;
         int idx = -1;
-        for (int k = 0; k < 4; ++k) {
-            if (cosv[k] < (T)0) {
-                const T *pl = plane(ph.tet, k);
-                T perp = dot3<T>(pl[0], pl[1], pl[2], ph.x, ph.y, ph.z) + pl[3];
-                T t = Num<T>::div(-perp, cosv[k]);
-                if (t < min_d) {
-                    min_d = t;
-                    idx = k;
-                    ph.min_cos = cosv[k];
+        if (kFused<T>) {
+            // FP32 forms: the nearest face by comparing perp_i / c_i against
+            // perp_j / c_j as perp_i * c_j < perp_j * c_i (c = -cos > 0),
+            // then one division for the winner.
+            T best_perp = 0, best_c = 0;
+            for (int k = 0; k < 4; ++k) {
+                if (cosv[k] < (T)0) {
+                    const T *pl = plane(ph.tet, k);
+                    const T perp = dot3<T>(pl[0], pl[1], pl[2], ph.x, ph.y, ph.z) + pl[3];
+                    const T c = -cosv[k];
+                    const bool nearer = idx < 0 ? perp < Num<T>::big * c
+                                                : perp * best_c < best_perp * c;
+                    if (nearer) {
+                        best_perp = perp;
+                        best_c = c;
+                        idx = k;
+                    }
+                }
+            }
+            if (idx >= 0) {
+                min_d = Num<T>::div(best_perp, best_c);
+                ph.min_cos = -best_c;
+            }
+        } else {
+            for (int k = 0; k < 4; ++k) {
+                if (cosv[k] < (T)0) {
+                    const T *pl = plane(ph.tet, k);
+                    T perp = dot3<T>(pl[0], pl[1], pl[2], ph.x, ph.y, ph.z) + pl[3];
+                    T t = Num<T>::div(-perp, cosv[k]);
+                    if (t < min_d) {
+                        min_d = t;
+                        idx = k;
+                        ph.min_cos = cosv[k];
+                    }
                 }
             }
         }
@@ -435,26 +467,34 @@ struct Lane {
         const T ni = S.regions[S.region[ph.tet]].n;
         const int next = S.adj[4 * ph.tet + ph.next_face];
         const T nt = next == -1 ? S.n_ambient : S.regions[S.region[next]].n;
-        const T ni_nt = Num<T>::div(ni, nt);
+        T r;
         T sa1 = std::sqrt(Num<T>::mad(-ca1, ca1, (T)1));
         if (ca1 > Num<T>::coszero) sa1 = 0;
-        const T sa2 = std::fmin(ni_nt * sa1, (T)1);
-        const T ca2 = std::sqrt(Num<T>::mad(-sa2, sa2, (T)1));
-        const T ca1ca2 = ca1 * ca2;
-        const T sa1sa2 = sa1 * sa2;
-        T sa1ca2 = sa1 * ca2;
-        T ca1sa2 = ca1 * sa2;
-        if (ca1 > Num<T>::coszero) {
-            sa1ca2 = 1;
-            ca1sa2 = ni_nt;
+        if (kFused<T> && ni == nt) {
+            // FP32 forms, matched refractive indices: Fresnel's R is exactly
+            // 0 (the formula only adds rounding noise in FP32), except for
+            // the reference's grazing-incidence rule (sa2 = sa1 here).
+            r = (ca1 < Num<T>::cos90 || sa1 == (T)1) ? (T)1 : (T)0;
+        } else {
+            const T ni_nt = Num<T>::div(ni, nt);
+            const T sa2 = std::fmin(ni_nt * sa1, (T)1);
+            const T ca2 = std::sqrt(Num<T>::mad(-sa2, sa2, (T)1));
+            const T ca1ca2 = ca1 * ca2;
+            const T sa1sa2 = sa1 * sa2;
+            T sa1ca2 = sa1 * ca2;
+            T ca1sa2 = ca1 * sa2;
+            if (ca1 > Num<T>::coszero) {
+                sa1ca2 = 1;
+                ca1sa2 = ni_nt;
+            }
+            const T cam = ca1ca2 + sa1sa2;
+            const T sap = sa1ca2 + ca1sa2;
+            const T sam = sa1ca2 - ca1sa2;
+            r = Num<T>::div(sam, sap * cam);
+            r = r * r;
+            r = r * Num<T>::mad(ca1ca2, ca1ca2, sa1sa2 * sa1sa2);
+            if (ca1 < Num<T>::cos90 || sa2 == (T)1) r = 1;
         }
-        const T cam = ca1ca2 + sa1sa2;
-        const T sap = sa1ca2 + ca1sa2;
-        const T sam = sa1ca2 - ca1sa2;
-        T r = Num<T>::div(sam, sap * cam);
-        r = r * r;
-        r = r * Num<T>::mad(ca1ca2, ca1ca2, sa1sa2 * sa1sa2);
-        if (ca1 < Num<T>::cos90 || sa2 == (T)1) r = 1;
 
         const T *pl = plane(ph.tet, ph.next_face);
         const T two_ca1 = ca1 + ca1;
@@ -548,10 +588,13 @@ struct Lane {
             else ph.uz = cost * (uz >= (T)0 ? (T)1 : (T)-1);
         } else {
             // RSQRT(x) taken as 1/sqrt(x), both correctly rounded.
-            const T temp = (T)1 / std::sqrt(Num<T>::mad(-uz, uz, (T)1));
+            const T sq = std::sqrt(Num<T>::mad(-uz, uz, (T)1));
+            const T temp = (T)1 / sq;
             ph.ux = Num<T>::mad(Num<T>::mad(stcp * ux, uz, -(stsp * uy)), temp, ux * cost);
             ph.uy = Num<T>::mad(Num<T>::mad(stcp * uy, uz, stsp * ux), temp, uy * cost);
-            ph.uz = Num<T>::mad(uz, cost, Num<T>::div(-stcp, temp));
+            // FAST_DIV(-stcp, temp) is -stcp * sqrt(1 - uz^2): the FP32 forms
+            // multiply, the FP64 form divides as the reference.
+            ph.uz = Num<T>::mad(uz, cost, kFused<T> ? -(stcp * sq) : Num<T>::div(-stcp, temp));
         }
     }
 
@@ -581,15 +624,26 @@ struct Lane {
         T vy = S.probe_y - ph.y;
         T vz = S.probe_z - ph.z;
         const T len = std::sqrt(Num<T>::mad(vz, vz, Num<T>::mad(vx, vx, vy * vy)));
-        vx = Num<T>::div(vx, len);
-        vy = Num<T>::div(vy, len);
-        vz = Num<T>::div(vz, len);
+        if (kFused<T>) {
+            // FP32 forms: one reciprocal, three products
+            const T rl = (T)1 / len;
+            vx *= rl;
+            vy *= rl;
+            vz *= rl;
+        } else {
+            vx = Num<T>::div(vx, len);
+            vy = Num<T>::div(vy, len);
+            vz = Num<T>::div(vz, len);
+        }
         if ((ph.fst_flag || ph.num_back > 0) && !reached) {
             reached = 2;
             const Region<T, P> &rg = S.regions[S.region[ph.tet]];
-            const T next_step = Num<T>::div(-Num<T>::log(S.rnd_step), rg.muas);
+            // -log(0)/mu_t is +infinity: with rndStepSizeInTissue = 0 (what the
+            // reference reads, src/octmps.h:124) the distance test always holds.
+            const bool far = S.rnd_step == (T)0 ||
+                             Num<T>::div(-Num<T>::log(S.rnd_step), rg.muas) >= len;
             // the distance to the probe equals len (same terms, same order)
-            if (next_step >= len && -vz >= S.cos_collect) reached = 1;
+            if (far && -vz >= S.cos_collect) reached = 1;
             btmp = S.bias_a;
         }
         int sel = 0;
