@@ -174,6 +174,7 @@ def run_ours(args, rank, world, local_rank, dist):
                for k in sel]
         ctx.flush()
         ts = [ctx.fetch(j, nb) for j in ids]
+        ctx.synchronize()  # the launch's device time is known once it has ended
         sts = [ctx.stats(j) for j in ids]
         for j in ids:
             ctx.release(j)

@@ -165,8 +165,10 @@ typedef struct {
     uint64_t packets;     /* packets launched (equals n_photons) */
     uint64_t steps;       /* propagation steps taken */
     uint64_t restores;    /* split copies resumed */
-    double device_ms;     /* kernel time of the launch that ran the job */
+    double device_ms;     /* kernel time of the launch the job finished in, or -1
+                             while that launch still runs (never waits) */
     double submit_to_done_ms;
+    int64_t launch_id;    /* sequence number (per context) of that launch */
 } octmps_job_stats;
 
 /* ---- context ------------------------------------------------------------ */
@@ -185,11 +187,15 @@ typedef struct {
     int32_t block_size;       /* threads per block */
     int32_t blocks_per_sm;    /* resident blocks per SM */
     int32_t default_lanes;    /* RNG lanes per job when job.n_lanes = 0 */
-    int32_t use_graphs;       /* replay launches through a CUDA graph */
+    int32_t use_graphs;       /* reserved, 0 (a batch is one persistent launch, so
+                                 there is no launch sequence to replay) */
     uint64_t hbm_budget_bytes;/* admission budget for job state; 0 = 80% of free */
     int32_t scatter_share;    /* a warp runs its lanes' scattering step halves once at
                                  least scatter_share/32 of its live lanes wait for one
                                  (1..32; 0 = 16) */
+    int32_t linger_us;        /* a kernel thread that finds no work waits this long for
+                                 newly submitted jobs before it exits (0 = 2000;
+                                 -1 = exit at once; at most 1000000) */
 } octmps_launch_config;
 octmps_status octmps_ctx_configure(octmps_ctx *ctx, const octmps_launch_config *cfg);
 
@@ -210,14 +216,44 @@ octmps_status octmps_rng_init(const uint32_t *multipliers, uint64_t n_multiplier
                               uint64_t seed, octmps_rng_lanes *out);
 
 /* ---- jobs ------------------------------------------------------------------
- * Submitted jobs queue up; octmps_ctx_flush (or a wait on any pending job)
- * runs every queued job in one persistent launch. */
+ * A job is one A-scan; the reference runs one per worker call (RunGPUi,
+ * src/main.cu:43).  Submitted jobs go into a device job table (one per
+ * precision); octmps_ctx_flush (or a wait on any job) starts a persistent
+ * launch over the table if none runs.  A job submitted while a launch runs
+ * is appended to the table and taken up by that launch as its threads free
+ * up (continuous batching); a job is finished, and can be fetched and
+ * released, as soon as all of its lanes have reported, which can be before
+ * the launch ends.  octmps_ctx_synchronize waits for every launch to end.
+ * octmps_ctx_poll is a completion queue: it advances the launches and
+ * returns up to max_ids jobs finished since the last poll (the first poll
+ * also returns jobs finished before it), without waiting. */
 octmps_status octmps_job_submit(octmps_ctx *ctx, const octmps_job *job, octmps_job_id *out);
 octmps_status octmps_ctx_flush(octmps_ctx *ctx);
+octmps_status octmps_ctx_synchronize(octmps_ctx *ctx);
+octmps_status octmps_ctx_poll(octmps_ctx *ctx, octmps_job_id *done, int32_t max_ids,
+                              int32_t *n_done);
 octmps_status octmps_job_wait(octmps_ctx *ctx, octmps_job_id id, int32_t timeout_ms);
 octmps_status octmps_job_fetch(octmps_ctx *ctx, octmps_job_id id, octmps_tally *out);
 octmps_status octmps_job_fetch_stats(octmps_ctx *ctx, octmps_job_id id, octmps_job_stats *out);
 octmps_status octmps_job_release(octmps_ctx *ctx, octmps_job_id id);
+
+/* Diagnosis: the first packet of a precision's job table (its current batch,
+ * else the latest batch that had one) that was stopped at the step cap (2^26
+ * steps; the reference has no cap), with the state it was stopped in; seed,
+ * n_lanes and n_photons are filled while the job is not released.
+ * stopped = 0 if none. */
+typedef struct {
+    int32_t stopped;
+    int32_t tet;
+    octmps_job_id job;
+    uint64_t seed, n_lanes, n_photons;
+    uint64_t lane;          /* RNG lane (virtual thread) of the job */
+    uint64_t packets_left;  /* packets of that lane still to run, this one included */
+    uint64_t steps;
+    double pos[3], dir[3];
+    double weight, step_left;
+} octmps_incident;
+octmps_status octmps_debug_incident(octmps_ctx *ctx, int32_t precision, octmps_incident *out);
 
 /* ---- files (the reference's formats) -------------------------------------- */
 octmps_status octmps_read_opt(const char *path, octmps_sim *out);

@@ -5,6 +5,8 @@
 
 #include <cstdint>
 
+#include <vector_types.h>
+
 namespace octmps {
 
 // Neighbour entry of the packed mesh: -1 for the ambient medium, else the
@@ -21,7 +23,11 @@ struct RegionConst {
 };
 
 // One job (one A-scan) of a launch.  All pointers are device pointers.
-struct JobDesc {
+// A slot is exactly two 128-byte cache lines of its own: a launch reads a
+// slot that the host filled while the launch ran, and no line of it may have
+// been cached in L1 before (a line shared with the neighbouring slot would
+// be, stale).
+struct alignas(256) JobDesc {
     const void *planes;   // per tet 4 inward planes (nx, ny, nz, d), float or double
     const int32_t *adj;   // per tet 4 packed neighbour entries (int4-aligned)
     const void *regions;  // RegionConst<T>[n_regions]
@@ -46,6 +52,8 @@ struct JobDesc {
     double shift, bin_width, half_lc;  // OpticalDepthShift, Lc/6, Lc/2 (round-down)
     int32_t root_tet, root_region, type_bias, nbins;
 };
+
+static_assert(sizeof(JobDesc) == 256, "a job slot is two cache lines");
 
 // Tally block of one job (P = double or float):
 //   uint64 totals[4]     NumFilteredPhotons, ...ClassI, ...ClassII, pad
@@ -82,16 +90,47 @@ OCTMPS_HD inline TallyLayout tally_layout(int nbins, size_t psize) {
     return L;
 }
 
+// The first packet a table's launches stopped at the step cap, for
+// diagnosis (written once; cleared when the table is reset).
+struct Incident {
+    unsigned int flag;
+    unsigned int slot;
+    int32_t tet;
+    uint32_t packets_left;  // packets of the lane still to run, this one included
+    uint64_t lane;
+    uint64_t steps;
+    double pos[3], dir[3];
+    double w, sleft;
+};
+
+// A launch works through a job table that may grow while it runs: the host
+// fills a free slot (descriptor and unit base) and only then raises the
+// total number of units, so a kernel thread that takes unit u < total always
+// finds u's slot complete.  Threads take units by compare-and-swap on the
+// next-unit counter, which therefore never passes the total.  A thread that
+// finds no unit left retries for linger_us (jobs submitted meanwhile are
+// taken up by the running launch) and then exits.  Several launches may work
+// through one table at once: the host starts another when work arrives while
+// the running one may be down to its last threads, and the new launch's
+// blocks take SM slots as the older launch's blocks leave.
 struct LaunchArgs {
-    const JobDesc *jobs;
-    const uint64_t *unit_base;  // [n_jobs+1]: first work unit (RNG lane) of each job
-    int32_t n_jobs;
-    uint64_t total_units;
-    unsigned long long *next_unit;  // work counter, zeroed before the launch
-    unsigned int *error;            // error word, zeroed before the launch
+    const JobDesc *jobs;            // job slots
+    const uint64_t *unit_base;      // [n_slots]: first unit of each slot; ~0 for empty slots
+    int32_t n_slots;                // table capacity (binary search range)
+    unsigned long long *ctrl;       // [0] next unit to hand out, [1] total units, [2] error word
+    uint2 *slot_state;              // per slot: x = units (RNG lanes) finished, y = launch_seq
+                                    // of the launch that finished the last one; may be null
+    Incident *incident;             // may be null
+    uint64_t start_unit;            // at launch thread t takes unit start_unit + t ...
+    uint64_t initial_total;         // ... if that is below the total at launch; 0 for a
+                                    // launch beside a running one (blocks claim runs)
     uint64_t step_cap;              // steps allowed per packet
     int32_t scatter_share;          // a warp runs the scattering halves of its steps once
                                     // at least scatter_share/32 of its live lanes wait
+    uint32_t launch_seq;            // nonzero
+    int32_t record_slot;            // recording variant: the slot whose lanes are recorded
+    uint32_t linger_us;             // a thread that finds no unit retries for this long
+                                    // (about 1 us granularity) before it exits
 };
 
 // Error bits reported through LaunchArgs::error.

@@ -33,8 +33,7 @@ namespace {
 // Scratch layout inside the array (offsets in bytes).
 constexpr size_t kJobOff = 0;                                        // JobDesc
 constexpr size_t kUnitOff = 512;                                     // uint64 unit_base[2]
-constexpr size_t kCounterOff = 544;                                  // work counter (u64)
-constexpr size_t kErrorOff = 552;                                    // error word (u32)
+constexpr size_t kCtrlOff = 544;     // u64 next unit, total units, error word
 constexpr size_t kStatsOff = 576;                                    // u64 stats[4]
 constexpr size_t kRegionOff = 640;                                   // RegionConst<float>[...]
 constexpr size_t kScratchBytes = kRegionOff + OCTMPS_NOALLOC_MAX_REGIONS * sizeof(RegionConst<float>);
@@ -151,7 +150,19 @@ extern "C" octmps_status octmps_ascan_run_noalloc(const octmps_noalloc_ascan *a,
     uint64_t *ub = reinterpret_cast<uint64_t *>(img + kUnitOff);
     ub[0] = 0;
     ub[1] = a->n_lanes;
-    // counter, error word and statistics start at zero (img is zeroed)
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        return OCTMPS_ERR_DEVICE;
+    int regs = 0, per_sm = 0;
+    if (photon_kernel_attributes(kMixed, 256, 2, &regs, &per_sm) != 0 || per_sm < 1) per_sm = 1;
+    uint64_t grid = (uint64_t)sms * per_sm;
+    const uint64_t useful = (a->n_lanes + 255) / 256;
+    if (grid > useful) grid = useful;
+    // thread t runs unit t first; the counter starts past those units
+    uint64_t *ctrl = reinterpret_cast<uint64_t *>(img + kCtrlOff);
+    ctrl[0] = grid * 256 < a->n_lanes ? grid * 256 : a->n_lanes;
+    ctrl[1] = a->n_lanes;
+    // error word and statistics start at zero (img is zeroed)
 
     if (cudaMemcpyAsync(scratch, img, sizeof img, cudaMemcpyHostToDevice, st) != cudaSuccess)
         return OCTMPS_ERR_DEVICE;
@@ -162,24 +173,21 @@ extern "C" octmps_status octmps_ascan_run_noalloc(const octmps_noalloc_ascan *a,
     LaunchArgs L;
     L.jobs = reinterpret_cast<const JobDesc *>(scratch + kJobOff);
     L.unit_base = reinterpret_cast<const uint64_t *>(scratch + kUnitOff);
-    L.n_jobs = 1;
-    L.total_units = a->n_lanes;
-    L.next_unit = reinterpret_cast<unsigned long long *>(scratch + kCounterOff);
-    L.error = reinterpret_cast<unsigned int *>(scratch + kErrorOff);
+    L.n_slots = 1;
+    L.ctrl = reinterpret_cast<unsigned long long *>(scratch + kCtrlOff);
+    L.slot_state = nullptr;
+    L.incident = nullptr;
+    L.start_unit = 0;
+    L.initial_total = a->n_lanes;
     L.step_cap = 1ull << 26;
     L.scatter_share = 10;
-    int sms = 0;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
-        return OCTMPS_ERR_DEVICE;
-    int regs = 0, per_sm = 0;
-    if (photon_kernel_attributes(kMixed, 256, 2, &regs, &per_sm) != 0 || per_sm < 1) per_sm = 1;
-    uint64_t grid = (uint64_t)sms * per_sm;
-    const uint64_t useful = (a->n_lanes + 255) / 256;
-    if (grid > useful) grid = useful;
+    L.launch_seq = 1;
+    L.record_slot = -1;
+    L.linger_us = 0;
     if (launch_photon_kernel(kMixed, 2, L, (int)grid, 256, st, nullptr) != 0)
         return OCTMPS_ERR_DEVICE;
     unsigned int err = 0;
-    if (cudaMemcpyAsync(&err, L.error, sizeof err, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+    if (cudaMemcpyAsync(&err, scratch + kCtrlOff + 16, sizeof err, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return OCTMPS_ERR_DEVICE;
     return err ? OCTMPS_ERR_KERNEL : OCTMPS_OK;

@@ -93,6 +93,66 @@ __device__ __forceinline__ unsigned long long fnv(unsigned long long h, unsigned
     return h;
 }
 
+constexpr uint32_t kRetryUs = 8;         // first retry interval of a thread waiting for work
+constexpr uint32_t kRetryMaxUs = 512;    // the interval doubles up to this
+constexpr unsigned kIdleSleepNs = 4000;  // pause of a warp whose lanes all wait
+
+// Global timer in ticks of 1.024 us (wraps after about 73 minutes; only
+// differences are used).
+__device__ __forceinline__ uint32_t timer_us() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return (uint32_t)(t >> 10);
+}
+
+// Claims up to k >= 1 units from the shared counter by compare-and-swap;
+// returns how many it got (0 when none is left) and the first in u.  Retries
+// back off (32 ns doubling to 1 us); after 2^20 failed tries it gives up,
+// which leaves the units to a later launch.
+__device__ __forceinline__ unsigned claim_units(unsigned long long *ctrl, unsigned k,
+                                                unsigned long long &u) {
+    unsigned ns = 32;
+    for (int attempt = 0; attempt < (1 << 20); ++attempt) {
+        const unsigned long long cur = __ldcv(ctrl);
+        const unsigned long long tot = __ldcv(ctrl + 1);
+        if (cur >= tot) return 0;
+        const unsigned long long c = min((unsigned long long)k, tot - cur);
+        if (atomicCAS(ctrl, cur, cur + c) == cur) {
+            u = cur;
+            return (unsigned)c;
+        }
+        __nanosleep(ns);
+        if (ns < 1024) ns <<= 1;
+    }
+    return 0;
+}
+
+// One unit for each lane of the warp that arrives here, claimed together by
+// the lowest such lane (one compare-and-swap per warp instead of per thread).
+__device__ __forceinline__ bool take_unit(unsigned long long *ctrl, unsigned long long &u) {
+    const unsigned m = __activemask();
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    const unsigned rank = __popc(m & ((1u << lane) - 1u));
+    unsigned long long base = 0;
+    unsigned c = 0;
+    if (lane == leader) c = claim_units(ctrl, __popc(m), base);
+    c = __shfl_sync(m, c, leader);
+    base = __shfl_sync(m, base, leader);
+    u = base + rank;
+    return rank < c;
+}
+
+// Reports a finished unit of a slot; the launch that finishes the slot's
+// last unit stamps its sequence number.  The unit's tallies are made visible
+// before the count.
+__device__ __forceinline__ void unit_finished(const LaunchArgs &args, int slot, uint32_t n_units) {
+    if (!args.slot_state) return;
+    __threadfence();
+    const unsigned before = atomicAdd(&args.slot_state[slot].x, 1u);
+    if (before + 1 == n_units) atomicExch(&args.slot_state[slot].y, args.launch_seq);
+}
+
 template <typename P>
 __device__ __forceinline__ void atomic_max_bits(P *addr, P v);
 template <>
@@ -614,23 +674,79 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     unsigned live = 0xffffffffu;
     bool pending = false;
     const int share = args.scatter_share;
+    unsigned int *const err = reinterpret_cast<unsigned int *>(args.ctrl + 2);
+    int slot = 0;  // job slot of the current unit
+    // First units: in a launch started on an idle table, thread t takes unit
+    // start_unit + t; in one started beside a running launch, each block
+    // claims a run of units at once (a grid's worth of threads arriving
+    // together would otherwise contend for the counter one by one).
+    __shared__ unsigned long long s_first;
+    __shared__ unsigned s_count;
+    unsigned long long first_u;
+    bool first_ok;
+    if (args.initial_total == 0) {
+        if (threadIdx.x == 0) {
+            s_first = 0;
+            s_count = claim_units(args.ctrl, kBlock, s_first);
+        }
+        __syncthreads();
+        first_u = s_first + threadIdx.x;
+        first_ok = threadIdx.x < s_count;
+    } else {
+        first_u = args.start_unit + (blockIdx.x * (unsigned long long)kBlock + threadIdx.x);
+        first_ok = first_u < args.initial_total;
+    }
+    bool first_unit = true;
+    // A thread that finds no unit left waits for jobs appended while the
+    // launch runs: it retries after kRetryUs, doubling the interval up to
+    // kRetryMaxUs (the counter's cache line is shared by every waiting warp),
+    // and exits after linger_us without a unit (times from the global timer
+    // in 1.024 us ticks).
+    bool waiting = false;
+    uint32_t idle_since = 0, last_try = 0, gap = kRetryUs;
 
     for (;;) {
         bool has_work = true;
         bool idle = false;
         if (packets_left == 0) {
-            const unsigned long long u = atomicAdd(args.next_unit, 1ull);
-            if (u >= args.total_units) {
-                has_work = false;
-            } else {
-                int lo = 0, hi = args.n_jobs - 1;
+            unsigned long long u = 0;
+            bool got = false;
+            if (first_unit) {
+                first_unit = false;
+                u = first_u;
+                got = first_ok;
+            }
+            if (!got) {
+                const uint32_t now = timer_us();
+                if (!waiting || now - last_try >= gap) {
+                    got = take_unit(args.ctrl, u);
+                    last_try = now;
+                    if (waiting && gap < kRetryMaxUs) gap <<= 1;
+                }
+                if (!got) {
+                    if (!waiting) {
+                        waiting = true;
+                        idle_since = now;
+                    }
+                    if (now - idle_since >= args.linger_us) has_work = false;
+                    else idle = true;
+                }
+            }
+            if (got) {
+                waiting = false;
+                gap = kRetryUs;
+                // the slot holding unit u: the last one whose base is <= u
+                // (bases of empty slots are ~0); read past L1, the host may
+                // have filled the slot after this launch started
+                int lo = 0, hi = args.n_slots - 1;
                 while (lo < hi) {
                     const int mid = (lo + hi + 1) >> 1;
-                    if (__ldg(args.unit_base + mid) <= u) lo = mid;
+                    if (__ldcg(args.unit_base + mid) <= u) lo = mid;
                     else hi = mid - 1;
                 }
+                slot = lo;
                 const JobDesc *jd = args.jobs + lo;
-                const uint64_t v = u - __ldg(args.unit_base + lo);
+                const uint64_t v = u - __ldcg(args.unit_base + lo);
                 if (jd != L.jd) {
                     L.jd = jd;
                     L.regions = reinterpret_cast<const RegionConst<T> *>(jd->regions);
@@ -652,11 +768,12 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
                 packets_left = (uint32_t)(jd->n_photons / nl + (v < jd->n_photons % nl ? 1 : 0));
                 if (packets_left == 0) {
                     idle = true;  // a lane without packets: take another unit next time
+                    unit_finished(args, slot, jd->n_lanes);
                 } else {
                     L.launch();
                     steps_packet = 0;
                     pending = false;
-                    recording = kRecord && records && lo == 0;
+                    recording = kRecord && records && lo == args.record_slot;
                     record_lane = v;
                 }
             }
@@ -668,6 +785,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
         const unsigned pend = __ballot_sync(live, pending && !idle);
         const unsigned ready = __ballot_sync(live, !pending && !idle);
         const bool run_b = ready == 0u || __popc(pend) * 32 >= share * __popc(live);
+        if ((pend | ready) == 0u) __nanosleep(kIdleSleepNs);  // every live lane waits for work
         if (idle) continue;
         bool end;
         if (run_b) {
@@ -676,7 +794,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
             end = L.phase_b(cont);
         } else {
             if (pending) continue;
-            const int r = L.phase_a(cont, args.error);
+            const int r = L.phase_a(cont, err);
             if (r == kPending) {
                 pending = true;
                 continue;
@@ -686,9 +804,25 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
         ++steps_packet;
         bool done = end;
         if (!done && steps_packet >= args.step_cap) {
-            atomicOr(args.error, kErrStepCap);
+            atomicOr(err, kErrStepCap);
             atomicAdd(&L.jd->stats[3], 1ull);
             done = true;
+            Incident *inc = args.incident;
+            if (inc && atomicCAS(&inc->flag, 0u, 1u) == 0u) {
+                inc->slot = (unsigned)slot;
+                inc->tet = L.tet;
+                inc->packets_left = packets_left;
+                inc->lane = record_lane;
+                inc->steps = steps_packet;
+                inc->pos[0] = (double)L.x;
+                inc->pos[1] = (double)L.y;
+                inc->pos[2] = (double)L.z;
+                inc->dir[0] = (double)L.ux;
+                inc->dir[1] = (double)L.uy;
+                inc->dir[2] = (double)L.uz;
+                inc->w = (double)L.w;
+                inc->sleft = (double)L.sleft;
+            }
         }
         if (done) {
             // per-packet statistics: steps, split copies resumed, packets
@@ -717,6 +851,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
             if (packets_left) {
                 L.launch();
                 steps_packet = 0;
+            } else {
+                unit_finished(args, slot, L.jd->n_lanes);
             }
         }
     }

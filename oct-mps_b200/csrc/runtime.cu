@@ -1,13 +1,37 @@
-// C-ABI runtime: context, resident meshes, job queue, persistent launches.
+// C-ABI runtime: context, resident meshes, continuous batching of jobs.
 //
 // Replaces the reference's per-A-scan worker RunGPUi (src/main.cu:43-660).
 // The reference allocates ~50 device buffers, uploads the whole mesh and
 // frees everything again for every A-scan, then relaunches its kernel in
 // 50,000-step slices polled from the host.  Here a mesh is uploaded once
-// and stays resident until released; a job (one A-scan) owns only its
-// tally block and its RNG lanes (shared between jobs with the same seed and
-// lane count); every job queued when a launch starts runs in that one
-// persistent launch, which ends when the last packet of the last job ends.
+// and stays resident until released; a job (one A-scan) owns only its tally
+// block and its RNG lanes (shared between jobs with the same seed and lane
+// count).
+//
+// Jobs go into a device-resident job table per precision.  A persistent
+// launch works through the table's units (RNG lanes); a job submitted while
+// the launch runs is appended to the table and taken up by the running
+// kernel as its threads free up (continuous batching), so its work overlaps
+// the work already on the GPU.  A kernel thread that finds no unit left
+// waits (linger_us, retrying) for new jobs before it exits, so a stream of
+// submissions keeps one launch at full width.  A launch whose threads have
+// begun to leave may be down to a few of them; work arriving then also
+// starts another launch over the same table (up to kMaxLaunches at once,
+// each on its own stream), whose blocks take SM slots as the older launch's
+// blocks leave.  A job is finished when all of its lanes have reported back,
+// which can be well before the launch ends.  When every unit of the table
+// has been handed out and every launch has ended, the table is reset for the
+// next batch; jobs arriving while the table is full wait for that.
+//
+// Nothing on the submit path runs a kernel (device buffers are filled by
+// copies, not memsets): a kernel queued behind a persistent launch that holds
+// every SM would wait for that launch to end.
+//
+// Device memory released while a launch runs is freed only once no launch
+// runs (deferred frees).  A running launch may hold lines of that memory in
+// its SMs' L1 caches, which are not coherent; were the memory handed to a
+// new job's buffers in the same launch, its threads could read the stale
+// lines instead of the new job's data.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -16,6 +40,7 @@
 #include <cfloat>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -36,6 +61,12 @@ namespace {
 // the B-scan workload (2 blocks: 128-register cap, no spills).
 constexpr int kDefaultMinBlocks = 2;
 constexpr int kDefaultScatterShare = 16;
+constexpr int kTableSlots = 4096;       // jobs per table between resets
+constexpr int kMaxLaunches = 4;         // launches in flight per table
+constexpr double kRefreshMs = 0.2;      // slot states are read back at most this often
+constexpr int kDefaultLingerUs = 2000;  // idle kernel threads wait this long for new jobs
+constexpr size_t kCtrlBytes = 256;      // control words, then the incident record at word 8
+static_assert(8 * sizeof(unsigned long long) + sizeof(Incident) <= kCtrlBytes, "control area");
 
 double now_ms() {
     return std::chrono::duration<double, std::milli>(
@@ -62,37 +93,63 @@ struct RngDev {
     int refs = 0;
 };
 
-struct Launch;
+// One persistent launch of a table.
+struct LaunchRec {
+    cudaEvent_t start = nullptr, stop = nullptr;
+    bool ended = false;
+    float ms = 0;
+    int64_t seq = 0;
+    int stream = 0;
+    ~LaunchRec() {
+        if (start) cudaEventDestroy(start);
+        if (stop) cudaEventDestroy(stop);
+    }
+};
 
 struct Job {
     octmps_job_id id = 0;
     octmps_mesh_id mesh = 0;
     octmps_sim sim;
     int precision = 0;
-    double probe[3] = {0, 0, 0};
     int32_t root = 0;
     uint64_t n_photons = 0;
     uint64_t seed = 0;
     uint32_t n_lanes = 0;
     std::shared_ptr<RngDev> rng;
     void *regions = nullptr;   // RegionConst<T>[n_regions]
-    void *tally = nullptr;     // tally block
+    void *tally = nullptr;     // tally block + 4 statistics words
     unsigned long long *stats = nullptr;
     size_t tally_bytes = 0;
-    std::shared_ptr<Launch> launch;
+    int slot = -1;             // slot in its table, -1 while waiting for one
+    std::shared_ptr<LaunchRec> launch;  // launch that finished its last lane
     double t_submit = 0, t_done = 0;
     bool done = false;
     octmps_status status = OCTMPS_OK;
     JobDesc desc;
 };
 
-struct Launch {
-    void *buf = nullptr;  // jobs, unit_base, counter, error word
-    cudaEvent_t start = nullptr, stop = nullptr;
-    bool complete = false;
-    unsigned int error = 0;
-    float ms = 0;
-    unsigned int *error_host = nullptr;  // pinned
+// Device job table of one precision.
+struct Table {
+    int prec = 0;
+    cudaStream_t streams[kMaxLaunches] = {};
+    JobDesc *d_jobs = nullptr;
+    uint64_t *d_base = nullptr;            // [kTableSlots]
+    unsigned long long *d_ctrl = nullptr;  // next, total, error; incident at word 8
+    uint2 *d_state = nullptr;              // [kTableSlots] units finished, finishing launch
+    uint2 *h_state = nullptr;              // pinned copy of d_state[0, n_used)
+    unsigned long long *h_ctrl = nullptr;  // pinned copy of the control words
+    double state_at = -1e30;               // host time of the last copy
+    int n_used = 0;
+    uint64_t total = 0;                    // units appended
+    uint64_t total_at_launch = 0;          // total when the newest launch started
+    uint64_t next = 0;                     // units handed out (exact while none runs)
+    unsigned error = 0;                    // error word of this table's current batch
+    std::vector<octmps_job_id> slot_job;
+    std::deque<octmps_job_id> waiting;     // jobs waiting for a free slot
+    std::vector<std::shared_ptr<LaunchRec>> running;  // launches in flight
+    std::vector<std::shared_ptr<LaunchRec>> batch;    // launches since the last reset
+    Incident last_incident{};              // kept across resets
+    octmps_job_id incident_job = 0;
 };
 
 }  // namespace
@@ -100,20 +157,33 @@ struct Launch {
 struct octmps_ctx {
     int device = 0;
     int n_sm = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;  // uploads, downloads and table updates
     std::vector<uint32_t> multipliers;
     std::map<octmps_mesh_id, std::unique_ptr<MeshDev>> meshes;
     std::map<octmps_job_id, std::unique_ptr<Job>> jobs;
     std::map<std::pair<uint64_t, uint32_t>, std::shared_ptr<RngDev>> rng_cache;
-    std::vector<octmps_job_id> pending;
+    std::unique_ptr<Table> tables[3];
     octmps_mesh_id next_mesh = 1;
     octmps_job_id next_job = 1;
+    int64_t launches = 0;
     octmps_launch_config cfg;
     uint64_t budget = 0;
     uint64_t in_use = 0;
     std::string err;
     std::recursive_mutex mu;
     void *record_buf = nullptr;  // optional per-lane records of the next launch
+    bool completion_queue = false;         // on after the first octmps_ctx_poll
+    std::deque<octmps_job_id> completed;   // finished jobs not yet returned by a poll
+    // pinned host bytes of value 0x00 / 0xff that device buffers are filled
+    // from by copy; outgrown buffers are kept until the context is destroyed
+    // (freeing pinned memory waits for the device)
+    unsigned char *h_fill[2] = {nullptr, nullptr};
+    size_t h_fill_cap[2] = {0, 0};
+    std::vector<void *> h_fill_old;
+    std::vector<void *> deferred;  // device buffers to free once no launch runs
+    uint64_t deferred_bytes = 0;   // their share of the HBM budget
+    JobDesc *h_desc = nullptr;   // pinned staging (1 slot)
+    uint64_t *h_base = nullptr;  // pinned staging (2 words)
 };
 
 namespace {
@@ -132,6 +202,30 @@ octmps_status cuda_fail(octmps_ctx *c, cudaError_t e, const char *what) {
     do {                                                 \
         cudaError_t e_ = (call);                         \
         if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
+    } while (0)
+
+// Fills device bytes with 0x00 or 0xff (value 0 or 1) through the copy
+// engine on the context stream; the caller synchronises the stream.
+octmps_status fill_device(octmps_ctx *ctx, void *dst, int value, size_t bytes) {
+    if (bytes == 0) return OCTMPS_OK;
+    if (ctx->h_fill_cap[value] < bytes) {
+        const size_t cap = std::max<size_t>(bytes, 1 << 20);
+        void *p = nullptr;
+        CK(cudaMallocHost(&p, cap), "pinned fill buffer");
+        memset(p, value ? 0xff : 0x00, cap);
+        if (ctx->h_fill[value]) ctx->h_fill_old.push_back(ctx->h_fill[value]);
+        ctx->h_fill[value] = static_cast<unsigned char *>(p);
+        ctx->h_fill_cap[value] = cap;
+    }
+    CK(cudaMemcpyAsync(dst, ctx->h_fill[value], bytes, cudaMemcpyHostToDevice, ctx->stream),
+       "device fill");
+    return OCTMPS_OK;
+}
+
+#define FILL(dst, value, bytes)                                        \
+    do {                                                               \
+        octmps_status st_ = fill_device(ctx, (dst), (value), (bytes)); \
+        if (st_ != OCTMPS_OK) return st_;                              \
     } while (0)
 
 template <typename T>
@@ -160,21 +254,6 @@ double div_rd(double a, double b) {
     return q;
 }
 
-octmps_status finish_launch(octmps_ctx *ctx, const std::shared_ptr<Launch> &L) {
-    if (L->complete) return OCTMPS_OK;
-    cudaError_t e = cudaEventSynchronize(L->stop);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "launch");
-    cudaEventElapsedTime(&L->ms, L->start, L->stop);
-    L->error = *L->error_host;
-    L->complete = true;
-    cudaFreeAsync(L->buf, ctx->stream);
-    cudaFreeHost(L->error_host);
-    L->error_host = nullptr;
-    cudaEventDestroy(L->start);
-    cudaEventDestroy(L->stop);
-    return OCTMPS_OK;
-}
-
 octmps_status ensure_planes_d(octmps_ctx *ctx, MeshDev &m) {
     if (m.planes_d) return OCTMPS_OK;
     CK(cudaMallocAsync(&m.planes_d, m.planes_host.size() * sizeof(double), ctx->stream), "planes");
@@ -185,79 +264,307 @@ octmps_status ensure_planes_d(octmps_ctx *ctx, MeshDev &m) {
     return OCTMPS_OK;
 }
 
-octmps_status flush_locked(octmps_ctx *ctx) {
-    if (ctx->pending.empty()) return OCTMPS_OK;
-    // One launch per precision present in the queue.
-    for (int prec = 0; prec < 3; ++prec) {
-        std::vector<Job *> js;
-        for (octmps_job_id id : ctx->pending) {
-            Job *j = ctx->jobs[id].get();
-            if (j->precision == prec) js.push_back(j);
-        }
-        if (js.empty()) continue;
-        const int nj = (int)js.size();
-        auto L = std::make_shared<Launch>();
-        const size_t jobs_bytes = sizeof(JobDesc) * nj;
-        const size_t base_off = (jobs_bytes + 15) & ~size_t(15);
-        const size_t ctr_off = base_off + (((nj + 1) * sizeof(uint64_t) + 15) & ~size_t(15));
-        const size_t total = ctr_off + 16;
-        CK(cudaMallocAsync(&L->buf, total, ctx->stream), "launch buffer");
-        std::vector<unsigned char> hb(total, 0);
-        uint64_t *ub = reinterpret_cast<uint64_t *>(hb.data() + base_off);
-        uint64_t units = 0;
-        for (int k = 0; k < nj; ++k) {
-            memcpy(hb.data() + sizeof(JobDesc) * k, &js[k]->desc, sizeof(JobDesc));
-            ub[k] = units;
-            units += js[k]->n_lanes;
-        }
-        ub[nj] = units;
-        CK(cudaMemcpyAsync(L->buf, hb.data(), total, cudaMemcpyHostToDevice, ctx->stream),
-           "launch upload");
-        CK(cudaMallocHost(&L->error_host, sizeof(unsigned int)), "pinned");
-        *L->error_host = 0;
-        LaunchArgs a;
-        a.jobs = reinterpret_cast<const JobDesc *>(L->buf);
-        a.unit_base = reinterpret_cast<const uint64_t *>((char *)L->buf + base_off);
-        a.n_jobs = nj;
-        a.total_units = units;
-        a.next_unit = reinterpret_cast<unsigned long long *>((char *)L->buf + ctr_off);
-        a.error = reinterpret_cast<unsigned int *>((char *)L->buf + ctr_off + 8);
-        // A packet needs ~10^2-10^4 steps; a photon caught in degenerate
-        // geometry (stepping s = 0 around an edge) is stopped and flagged.
-        a.step_cap = 1ull << 26;
-        a.scatter_share = ctx->cfg.scatter_share > 0 ? ctx->cfg.scatter_share : kDefaultScatterShare;
-        // Variant compiled for 2 or 3 resident blocks per SM (register cap
-        // 128 or 80); the FP64 form has only the first.
-        int min_blocks = ctx->cfg.blocks_per_sm == 2 || ctx->cfg.blocks_per_sm == 3
-                             ? ctx->cfg.blocks_per_sm
-                             : kDefaultMinBlocks;
-        if (prec == kFP64 || ctx->record_buf) min_blocks = 2;
-        int regs = 0, per_sm = 0;
-        int st = photon_kernel_attributes(prec, 256, min_blocks, &regs, &per_sm);
-        if (st) return cuda_fail(ctx, (cudaError_t)st, "kernel attributes");
-        if (per_sm < 1) per_sm = 1;
-        const uint64_t max_useful = (units + 255) / 256;
-        int grid = ctx->n_sm * per_sm;
-        if ((uint64_t)grid > max_useful) grid = (int)std::max<uint64_t>(1, max_useful);
-        CK(cudaEventCreate(&L->start), "event");
-        CK(cudaEventCreate(&L->stop), "event");
-        CK(cudaEventRecord(L->start, ctx->stream), "event");
-        st = launch_photon_kernel(prec, min_blocks, a, grid, 256, ctx->stream, ctx->record_buf);
-        if (st) return cuda_fail(ctx, (cudaError_t)st, "photon kernel launch");
-        CK(cudaMemcpyAsync(L->error_host, a.error, sizeof(unsigned int), cudaMemcpyDeviceToHost,
-                           ctx->stream),
-           "error word");
-        CK(cudaEventRecord(L->stop, ctx->stream), "event");
-        for (Job *j : js) j->launch = L;
+octmps_status table_get(octmps_ctx *ctx, int prec, Table **out) {
+    std::unique_ptr<Table> &T = ctx->tables[prec];
+    if (!T) {
+        std::unique_ptr<Table> t(new Table());
+        t->prec = prec;
+        for (auto &s : t->streams)
+            CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+        const size_t jb = sizeof(JobDesc) * kTableSlots;
+        const size_t bb = sizeof(uint64_t) * kTableSlots;
+        const size_t sb = sizeof(uint2) * kTableSlots;
+        char *p = nullptr;
+        CK(cudaMalloc((void **)&p, jb + bb + kCtrlBytes + sb), "job table");
+        t->d_jobs = reinterpret_cast<JobDesc *>(p);
+        t->d_base = reinterpret_cast<uint64_t *>(p + jb);
+        t->d_ctrl = reinterpret_cast<unsigned long long *>(p + jb + bb);
+        t->d_state = reinterpret_cast<uint2 *>(p + jb + bb + kCtrlBytes);
+        CK(cudaMallocHost(&t->h_state, sb), "job table");
+        CK(cudaMallocHost(&t->h_ctrl, kCtrlBytes), "job table");
+        FILL(t->d_base, 1, bb);
+        FILL(t->d_ctrl, 0, kCtrlBytes + sb);
+        CK(cudaStreamSynchronize(ctx->stream), "job table");
+        T = std::move(t);
     }
-    ctx->pending.clear();
+    *out = T.get();
+    return OCTMPS_OK;
+}
+
+// Collects the table's ended launches; after any has ended, reads back the
+// control words (the next-unit counter is exact once none runs).
+octmps_status table_poll(octmps_ctx *ctx, Table &T) {
+    bool any = false;
+    for (size_t i = 0; i < T.running.size();) {
+        LaunchRec &L = *T.running[i];
+        cudaError_t q = cudaEventQuery(L.stop);
+        if (q == cudaErrorNotReady) {
+            ++i;
+            continue;
+        }
+        if (q != cudaSuccess) return cuda_fail(ctx, q, "photon kernel");
+        cudaEventElapsedTime(&L.ms, L.start, L.stop);
+        L.ended = true;
+        T.running.erase(T.running.begin() + i);
+        any = true;
+    }
+    if (!any) return OCTMPS_OK;
+    CK(cudaMemcpyAsync(T.h_ctrl, T.d_ctrl, 3 * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, ctx->stream),
+       "control words");
+    CK(cudaStreamSynchronize(ctx->stream), "control words");
+    T.next = T.h_ctrl[0];
+    T.error = (unsigned)T.h_ctrl[2];
+    return OCTMPS_OK;
+}
+
+// Starts a launch over the table: when none runs and units are left (its
+// threads first take the next units in order), or when units were appended
+// since the newest launch started (its blocks claim units from the shared
+// counter).
+octmps_status table_launch(octmps_ctx *ctx, Table &T) {
+    if (ctx->record_buf && !T.running.empty() && T.total > T.total_at_launch) {
+        // a recording launch runs alone, so that its threads (and no others)
+        // take the recorded job's units: wait for the running ones to end
+        for (auto &r : T.running) CK(cudaEventSynchronize(r->stop), "launch");
+        octmps_status st = table_poll(ctx, T);
+        if (st != OCTMPS_OK) return st;
+    }
+    const bool fresh = T.running.empty();
+    if (fresh ? T.next >= T.total
+              : (T.total <= T.total_at_launch || (int)T.running.size() >= kMaxLaunches))
+        return OCTMPS_OK;
+    // Variant compiled for 2 or 3 resident blocks per SM (register cap
+    // 128 or 80); the FP64 form and the recording variant have only 2.
+    int min_blocks = ctx->cfg.blocks_per_sm == 2 || ctx->cfg.blocks_per_sm == 3
+                         ? ctx->cfg.blocks_per_sm
+                         : kDefaultMinBlocks;
+    if (T.prec == kFP64 || ctx->record_buf) min_blocks = 2;
+    int regs = 0, per_sm = 0;
+    int st = photon_kernel_attributes(T.prec, 256, min_blocks, &regs, &per_sm);
+    if (st) return cuda_fail(ctx, (cudaError_t)st, "kernel attributes");
+    if (per_sm < 1) per_sm = 1;
+    const uint64_t grid = (uint64_t)ctx->n_sm * per_sm;
+    const uint64_t threads = grid * 256;
+    int si = 0;
+    while (si < kMaxLaunches) {
+        bool used = false;
+        for (auto &r : T.running) used |= r->stream == si;
+        if (!used) break;
+        ++si;
+    }
+    LaunchArgs a;
+    a.jobs = T.d_jobs;
+    a.unit_base = T.d_base;
+    a.n_slots = kTableSlots;
+    a.ctrl = T.d_ctrl;
+    a.slot_state = T.d_state;
+    a.incident = reinterpret_cast<Incident *>(T.d_ctrl + 8);
+    if (fresh) {
+        // thread t takes unit next + t; the counter starts past them (no
+        // launch runs, so the copy races with nothing)
+        T.h_ctrl[0] = std::min<uint64_t>(T.total, T.next + threads);
+        CK(cudaMemcpyAsync(T.d_ctrl, T.h_ctrl, sizeof(unsigned long long),
+                           cudaMemcpyHostToDevice, ctx->stream),
+           "control words");
+        CK(cudaStreamSynchronize(ctx->stream), "control words");
+        a.start_unit = T.next;
+        a.initial_total = T.total;
+    } else {
+        a.start_unit = 0;
+        a.initial_total = 0;
+    }
+    // A packet needs ~10^2-10^4 steps; a photon caught in degenerate
+    // geometry (stepping s = 0 around an edge) is stopped and flagged.
+    a.step_cap = 1ull << 26;
+    a.scatter_share = ctx->cfg.scatter_share > 0 ? ctx->cfg.scatter_share : kDefaultScatterShare;
+    a.linger_us = ctx->cfg.linger_us < 0    ? 0u
+                  : ctx->cfg.linger_us == 0 ? (uint32_t)kDefaultLingerUs
+                                            : (uint32_t)ctx->cfg.linger_us;
+    auto L = std::make_shared<LaunchRec>();
+    L->seq = ++ctx->launches;
+    L->stream = si;
+    a.launch_seq = (uint32_t)L->seq;
+    a.record_slot = T.n_used - 1;
+    cudaStream_t s = T.streams[si];
+    CK(cudaEventCreate(&L->start), "event");
+    CK(cudaEventCreate(&L->stop), "event");
+    CK(cudaEventRecord(L->start, s), "event");
+    st = launch_photon_kernel(T.prec, min_blocks, a, (int)grid, 256, s, ctx->record_buf);
+    if (st) return cuda_fail(ctx, (cudaError_t)st, "photon kernel launch");
+    CK(cudaEventRecord(L->stop, s), "event");
+    T.total_at_launch = T.total;
+    T.running.push_back(L);
+    T.batch.push_back(L);
     ctx->record_buf = nullptr;
     return OCTMPS_OK;
 }
 
+// Appends a job to a free slot: descriptor and unit base first, then the
+// total that makes the kernel hand out its units.
+octmps_status table_append(octmps_ctx *ctx, Table &T, Job &j) {
+    const int slot = T.n_used++;
+    j.slot = slot;
+    if ((int)T.slot_job.size() <= slot) T.slot_job.resize(slot + 1);
+    T.slot_job[slot] = j.id;
+    memcpy(ctx->h_desc, &j.desc, sizeof(JobDesc));
+    ctx->h_base[0] = T.total;
+    T.total += j.n_lanes;
+    ctx->h_base[1] = T.total;
+    CK(cudaMemcpyAsync(T.d_jobs + slot, ctx->h_desc, sizeof(JobDesc), cudaMemcpyHostToDevice,
+                       ctx->stream),
+       "job table");
+    CK(cudaMemcpyAsync(T.d_base + slot, ctx->h_base, sizeof(uint64_t), cudaMemcpyHostToDevice,
+                       ctx->stream),
+       "job table");
+    CK(cudaMemcpyAsync(T.d_ctrl + 1, ctx->h_base + 1, sizeof(uint64_t), cudaMemcpyHostToDevice,
+                       ctx->stream),
+       "job table");
+    CK(cudaStreamSynchronize(ctx->stream), "job table");
+    return OCTMPS_OK;
+}
+
+void mark_done(octmps_ctx *ctx, Job &j) {
+    j.done = true;
+    j.t_done = now_ms();
+    if (ctx->completion_queue) ctx->completed.push_back(j.id);
+}
+
+// Reads back every slot's state (units finished, finishing launch) and the
+// error word, and marks the jobs whose lanes have all reported as done.
+octmps_status table_refresh(octmps_ctx *ctx, Table &T) {
+    if (T.n_used == 0) return OCTMPS_OK;
+    CK(cudaMemcpyAsync(T.h_state, T.d_state, sizeof(uint2) * T.n_used, cudaMemcpyDeviceToHost,
+                       ctx->stream),
+       "job state");
+    CK(cudaMemcpyAsync(T.h_ctrl + 3, T.d_ctrl + 2, sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, ctx->stream),
+       "error word");
+    CK(cudaStreamSynchronize(ctx->stream), "job state");
+    T.state_at = now_ms();
+    const unsigned err = (unsigned)T.h_ctrl[3];
+    for (int s = 0; s < T.n_used; ++s) {
+        auto it = ctx->jobs.find(T.slot_job[s]);
+        if (it == ctx->jobs.end() || it->second->done) continue;
+        Job &j = *it->second;
+        const uint2 st = T.h_state[s];
+        // the finishing launch stamps its number just after the last count
+        if (st.x < j.n_lanes || st.y == 0) continue;
+        mark_done(ctx, j);
+        for (auto &L : T.batch)
+            if (L->seq == (int64_t)st.y) j.launch = L;
+        if (err) {
+            j.status = OCTMPS_ERR_KERNEL;
+            char msg[96];
+            snprintf(msg, sizeof msg, "kernel error word 0x%x", err);
+            ctx->err = msg;
+        }
+    }
+    return OCTMPS_OK;
+}
+
+// A table whose launches have all ended with every unit handed out holds
+// only finished jobs: they are marked done and the slots are freed.
+octmps_status table_try_reset(octmps_ctx *ctx, Table &T) {
+    if (!T.running.empty() || T.n_used == 0 || T.next < T.total) return OCTMPS_OK;
+    octmps_status st = table_refresh(ctx, T);
+    if (st != OCTMPS_OK) return st;
+    for (int s = 0; s < T.n_used; ++s) {
+        auto it = ctx->jobs.find(T.slot_job[s]);
+        if (it == ctx->jobs.end()) continue;
+        Job &j = *it->second;
+        if (!j.done) {  // cannot happen unless the kernel lost units
+            mark_done(ctx, j);
+            j.status = OCTMPS_ERR_KERNEL;
+            ctx->err = "job lanes missing at the end of the launches";
+        }
+        j.slot = -1;
+    }
+    // keep the incident record (if any) of the batch before clearing it
+    Incident inc;
+    CK(cudaMemcpyAsync(&inc, T.d_ctrl + 8, sizeof inc, cudaMemcpyDeviceToHost, ctx->stream),
+       "incident");
+    CK(cudaStreamSynchronize(ctx->stream), "incident");
+    if (inc.flag) {
+        T.last_incident = inc;
+        T.incident_job = (int)inc.slot < T.n_used ? T.slot_job[inc.slot] : 0;
+    }
+    FILL(T.d_base, 1, sizeof(uint64_t) * T.n_used);
+    FILL(T.d_state, 0, sizeof(uint2) * T.n_used);
+    FILL(T.d_ctrl, 0, kCtrlBytes);
+    CK(cudaStreamSynchronize(ctx->stream), "job table");
+    T.n_used = 0;
+    T.total = T.next = T.total_at_launch = 0;
+    T.error = 0;
+    T.slot_job.clear();
+    T.batch.clear();
+    // jobs that were waiting for a slot move in
+    while (!T.waiting.empty() && T.n_used < kTableSlots) {
+        auto it = ctx->jobs.find(T.waiting.front());
+        T.waiting.pop_front();
+        if (it == ctx->jobs.end()) continue;
+        st = table_append(ctx, T, *it->second);
+        if (st != OCTMPS_OK) return st;
+    }
+    return OCTMPS_OK;
+}
+
+// One scheduling round of a table: collect ended launches, free the table
+// if drained, launch if work is waiting.
+void free_deferred(octmps_ctx *ctx);
+
+octmps_status table_step(octmps_ctx *ctx, Table &T) {
+    octmps_status st = table_poll(ctx, T);
+    if (st != OCTMPS_OK) return st;
+    free_deferred(ctx);
+    st = table_try_reset(ctx, T);
+    if (st != OCTMPS_OK) return st;
+    return table_launch(ctx, T);
+}
+
+// Whether a job has finished: all of its lanes reported (read back from the
+// device while launches may still run).
+octmps_status job_check(octmps_ctx *ctx, Job &j) {
+    if (j.done) return OCTMPS_OK;
+    Table &T = *ctx->tables[j.precision];
+    octmps_status st = table_step(ctx, T);
+    if (st != OCTMPS_OK || j.done || j.slot < 0) return st;
+    if (now_ms() - T.state_at < kRefreshMs) return OCTMPS_OK;
+    return table_refresh(ctx, T);
+}
+
+void defer_free(octmps_ctx *ctx, void *p, uint64_t budget_bytes) {
+    if (!p) return;
+    ctx->deferred.push_back(p);
+    ctx->deferred_bytes += budget_bytes;
+}
+
+bool any_launch_running(octmps_ctx *ctx) {
+    for (auto &t : ctx->tables)
+        if (t && !t->running.empty()) return true;
+    return false;
+}
+
+// Frees the deferred buffers once no launch runs.
+void free_deferred(octmps_ctx *ctx) {
+    if (ctx->deferred.empty() || any_launch_running(ctx)) return;
+    for (void *p : ctx->deferred) cudaFreeAsync(p, ctx->stream);
+    ctx->deferred.clear();
+    ctx->deferred_bytes = 0;
+}
+
+void free_mesh_device(octmps_ctx *ctx, MeshDev &m) {
+    defer_free(ctx, m.planes_f, 0);
+    defer_free(ctx, m.planes_d, 0);
+    defer_free(ctx, m.adj, 0);
+    m.planes_f = m.planes_d = nullptr;
+    m.adj = nullptr;
+    free_deferred(ctx);
+}
+
 void release_job_device(octmps_ctx *ctx, Job *j) {
-    if (j->regions) cudaFreeAsync(j->regions, ctx->stream);
-    if (j->tally) cudaFreeAsync(j->tally, ctx->stream);
+    defer_free(ctx, j->regions, 0);
+    defer_free(ctx, j->tally, j->tally ? j->tally_bytes : 0);
     j->regions = nullptr;
     j->tally = nullptr;
     j->stats = nullptr;
@@ -270,7 +577,9 @@ void release_job_device(octmps_ctx *ctx, Job *j) {
                     break;
                 }
             if (j->rng.use_count() <= 1) {
-                cudaFreeAsync(j->rng->x, ctx->stream);
+                const uint64_t rb = (uint64_t)j->rng->n_lanes * 36;
+                defer_free(ctx, j->rng->x, rb);
+                ctx->in_use = ctx->in_use >= rb ? ctx->in_use - rb : 0;
             }
         }
         j->rng.reset();
@@ -279,12 +588,11 @@ void release_job_device(octmps_ctx *ctx, Job *j) {
     if (mi != ctx->meshes.end()) {
         MeshDev &m = *mi->second;
         if (--m.refs == 0 && m.released) {
-            cudaFreeAsync(m.planes_f, ctx->stream);
-            if (m.planes_d) cudaFreeAsync(m.planes_d, ctx->stream);
-            cudaFreeAsync(m.adj, ctx->stream);
+            free_mesh_device(ctx, m);
             ctx->meshes.erase(mi);
         }
     }
+    free_deferred(ctx);
 }
 
 }  // namespace
@@ -325,9 +633,21 @@ octmps_status octmps_ctx_create(int device, octmps_ctx **out) {
     if (cudaSetDevice(device) != cudaSuccess) return OCTMPS_ERR_DEVICE;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
         return OCTMPS_ERR_DEVICE;
+    if (cudaMallocHost(&c->h_desc, sizeof(JobDesc)) != cudaSuccess ||
+        cudaMallocHost(&c->h_base, 2 * sizeof(uint64_t)) != cudaSuccess)
+        return OCTMPS_ERR_OOM;
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
     c->budget = (uint64_t)(0.8 * (double)fr);
+    // Job buffers come from the device's stream-ordered pool.  Memory freed
+    // there stays mapped (no release threshold): handing it back to the
+    // driver at each synchronisation would unmap pages while a launch runs,
+    // which stalls the launch; the pool is bounded by the HBM budget anyway.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     *out = c.release();
     return OCTMPS_OK;
 }
@@ -337,12 +657,10 @@ octmps_status octmps_ctx_destroy(octmps_ctx *ctx) {
     {
         std::lock_guard<std::recursive_mutex> g(ctx->mu);
         cudaSetDevice(ctx->device);
+        for (auto &t : ctx->tables)
+            if (t)
+                for (auto s : t->streams) cudaStreamSynchronize(s);
         cudaStreamSynchronize(ctx->stream);
-        for (auto &kv : ctx->jobs) {
-            Job *j = kv.second.get();
-            if (j->launch) finish_launch(ctx, j->launch);
-            j->launch.reset();
-        }
         std::vector<octmps_job_id> ids;
         for (auto &kv : ctx->jobs) ids.push_back(kv.first);
         for (auto id : ids) release_job_device(ctx, ctx->jobs[id].get());
@@ -353,8 +671,25 @@ octmps_status octmps_ctx_destroy(octmps_ctx *ctx) {
             cudaFreeAsync(kv.second->adj, ctx->stream);
         }
         ctx->meshes.clear();
+        for (void *p : ctx->deferred) cudaFreeAsync(p, ctx->stream);  // every launch has ended
+        ctx->deferred.clear();
         cudaStreamSynchronize(ctx->stream);
+        for (auto &t : ctx->tables)
+            if (t) {
+                t->running.clear();
+                t->batch.clear();
+                cudaFree(t->d_jobs);
+                cudaFreeHost(t->h_state);
+                cudaFreeHost(t->h_ctrl);
+                for (auto s : t->streams) cudaStreamDestroy(s);
+                t.reset();
+            }
         cudaStreamDestroy(ctx->stream);
+        cudaFreeHost(ctx->h_desc);
+        cudaFreeHost(ctx->h_base);
+        for (void *p : ctx->h_fill)
+            if (p) cudaFreeHost(p);
+        for (void *p : ctx->h_fill_old) cudaFreeHost(p);
     }
     delete ctx;
     return OCTMPS_OK;
@@ -372,6 +707,10 @@ octmps_status octmps_ctx_configure(octmps_ctx *ctx, const octmps_launch_config *
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     if (cfg->block_size != 0 && cfg->block_size != 256)
         return fail(ctx, OCTMPS_ERR_INVALID_ARG, "block_size must be 256");
+    if (cfg->scatter_share < 0 || cfg->scatter_share > 32)
+        return fail(ctx, OCTMPS_ERR_INVALID_ARG, "scatter_share must be 0..32");
+    if (cfg->linger_us < -1 || cfg->linger_us > 1000000)
+        return fail(ctx, OCTMPS_ERR_INVALID_ARG, "linger_us must be -1..1000000");
     ctx->cfg = *cfg;
     if (cfg->hbm_budget_bytes) ctx->budget = cfg->hbm_budget_bytes;
     return OCTMPS_OK;
@@ -434,9 +773,7 @@ octmps_status octmps_mesh_release(octmps_ctx *ctx, octmps_mesh_id id) {
     if (it == ctx->meshes.end() || it->second->released) return OCTMPS_ERR_NOT_FOUND;
     it->second->released = true;
     if (it->second->refs == 0) {
-        cudaFreeAsync(it->second->planes_f, ctx->stream);
-        if (it->second->planes_d) cudaFreeAsync(it->second->planes_d, ctx->stream);
-        cudaFreeAsync(it->second->adj, ctx->stream);
+        free_mesh_device(ctx, *it->second);
         ctx->meshes.erase(it);
     }
     return OCTMPS_OK;
@@ -476,6 +813,11 @@ octmps_status octmps_job_submit(octmps_ctx *ctx, const octmps_job *job, octmps_j
     if (ctx->multipliers.size() < 3 + 3 * (uint64_t)lanes)
         return fail(ctx, OCTMPS_ERR_INVALID_ARG, "multiplier table too short for the lane count");
     const uint64_t seed = job->seed ? job->seed : 985456376ull;
+    Table *T = nullptr;
+    {
+        octmps_status st = table_get(ctx, job->precision, &T);
+        if (st != OCTMPS_OK) return st;
+    }
     if (job->precision == OCTMPS_PREC_FP64) {
         octmps_status st = ensure_planes_d(ctx, m);
         if (st != OCTMPS_OK) return st;
@@ -486,9 +828,6 @@ octmps_status octmps_job_submit(octmps_ctx *ctx, const octmps_job *job, octmps_j
     j->mesh = job->mesh;
     j->sim = s;
     j->precision = job->precision;
-    j->probe[0] = job->probe_x;
-    j->probe[1] = job->probe_y;
-    j->probe[2] = job->probe_z;
     j->root = job->root_tet;
     j->n_photons = n_ph;
     j->seed = seed;
@@ -504,7 +843,14 @@ octmps_status octmps_job_submit(octmps_ctx *ctx, const octmps_job *job, octmps_j
     auto ri = ctx->rng_cache.find(key);
     uint64_t need = j->tally_bytes;
     if (ri == ctx->rng_cache.end()) need += (uint64_t)lanes * 36;
-    if (ctx->in_use + need > ctx->budget)
+    // memory released while a launch runs counts until no launch runs
+    for (auto &t : ctx->tables)
+        if (t) {
+            octmps_status st = table_poll(ctx, *t);
+            if (st != OCTMPS_OK) return st;
+        }
+    free_deferred(ctx);
+    if (ctx->in_use + ctx->deferred_bytes + need > ctx->budget)
         return fail(ctx, OCTMPS_ERR_BUDGET, "job does not fit the HBM budget");
     if (ri != ctx->rng_cache.end()) {
         j->rng = ri->second;
@@ -535,6 +881,7 @@ octmps_status octmps_job_submit(octmps_ctx *ctx, const octmps_job *job, octmps_j
         CK(cudaMemcpyAsync(r->aS, haS.data(), n4, cudaMemcpyHostToDevice, ctx->stream), "rng");
         CK(cudaStreamSynchronize(ctx->stream), "rng upload");  // host vectors go out of scope
         ctx->rng_cache[key] = r;
+        ctx->in_use += (uint64_t)lanes * 36;
         j->rng = r;
     }
     j->rng->refs++;
@@ -547,7 +894,7 @@ octmps_status octmps_job_submit(octmps_ctx *ctx, const octmps_job *job, octmps_j
                        ctx->stream),
        "regions");
     CK(cudaMallocAsync(&j->tally, j->tally_bytes, ctx->stream), "tally");
-    CK(cudaMemsetAsync(j->tally, 0, j->tally_bytes, ctx->stream), "tally");
+    FILL(j->tally, 0, j->tally_bytes);
     CK(cudaStreamSynchronize(ctx->stream), "job upload");
     j->stats = reinterpret_cast<unsigned long long *>((char *)j->tally + stats_off);
     ctx->in_use += j->tally_bytes;
@@ -591,9 +938,16 @@ octmps_status octmps_job_submit(octmps_ctx *ctx, const octmps_job *job, octmps_j
     D.type_bias = s.type_bias;
     D.nbins = s.num_optical_depth_length_steps;
 
+    Job &jr = *j;
     *out = j->id;
-    ctx->pending.push_back(j->id);
     ctx->jobs[j->id] = std::move(j);
+    // Into the table now (a running launch takes it up), or into the queue
+    // of jobs waiting for a slot.
+    octmps_status st = table_poll(ctx, *T);
+    if (st == OCTMPS_OK) st = table_try_reset(ctx, *T);
+    if (st != OCTMPS_OK) return st;
+    if (T->n_used < kTableSlots && T->waiting.empty()) return table_append(ctx, *T, jr);
+    T->waiting.push_back(jr.id);
     return OCTMPS_OK;
 }
 
@@ -601,11 +955,102 @@ octmps_status octmps_ctx_flush(octmps_ctx *ctx) {
     if (!ctx) return OCTMPS_ERR_INVALID_ARG;
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     cudaSetDevice(ctx->device);
-    return flush_locked(ctx);
+    for (auto &t : ctx->tables) {
+        if (!t) continue;
+        octmps_status st = table_step(ctx, *t);
+        if (st != OCTMPS_OK) return st;
+    }
+    return OCTMPS_OK;
 }
 
-// Test hook: per-lane records of the first packets of the first job of the
-// next launch (device buffer of n_lanes records, 80 bytes each).
+octmps_status octmps_ctx_synchronize(octmps_ctx *ctx) {
+    if (!ctx) return OCTMPS_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    for (auto &t : ctx->tables) {
+        if (!t) continue;
+        octmps_status st = table_step(ctx, *t);
+        // a launch that ends with units left (jobs appended as its threads
+        // were leaving) is followed by another, which this waits for too
+        while (st == OCTMPS_OK && !t->running.empty()) {
+            CK(cudaEventSynchronize(t->running.front()->stop), "launch");
+            st = table_step(ctx, *t);
+        }
+        if (st != OCTMPS_OK) return st;
+    }
+    return OCTMPS_OK;
+}
+
+octmps_status octmps_ctx_poll(octmps_ctx *ctx, octmps_job_id *done, int32_t max_ids,
+                              int32_t *n_done) {
+    if (!ctx || !n_done || max_ids < 0 || (max_ids > 0 && !done)) return OCTMPS_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    *n_done = 0;
+    if (!ctx->completion_queue) {
+        // jobs that finished before the first poll are reported too
+        ctx->completion_queue = true;
+        for (auto &kv : ctx->jobs)
+            if (kv.second->done) ctx->completed.push_back(kv.first);
+    }
+    for (auto &t : ctx->tables) {
+        if (!t) continue;
+        octmps_status st = table_step(ctx, *t);
+        if (st == OCTMPS_OK && t->n_used > 0 && now_ms() - t->state_at >= kRefreshMs)
+            st = table_refresh(ctx, *t);
+        if (st != OCTMPS_OK) return st;
+    }
+    while (*n_done < max_ids && !ctx->completed.empty()) {
+        const octmps_job_id id = ctx->completed.front();
+        ctx->completed.pop_front();
+        if (ctx->jobs.count(id)) done[(*n_done)++] = id;
+    }
+    return OCTMPS_OK;
+}
+
+octmps_status octmps_debug_incident(octmps_ctx *ctx, int32_t precision, octmps_incident *out) {
+    if (!ctx || !out || precision < 0 || precision > 2) return OCTMPS_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    cudaSetDevice(ctx->device);
+    memset(out, 0, sizeof *out);
+    Table *T = ctx->tables[precision].get();
+    if (!T) return OCTMPS_OK;
+    Incident inc;
+    CK(cudaMemcpyAsync(&inc, T->d_ctrl + 8, sizeof inc, cudaMemcpyDeviceToHost, ctx->stream),
+       "incident");
+    CK(cudaStreamSynchronize(ctx->stream), "incident");
+    octmps_job_id jid = 0;
+    if (inc.flag) {
+        jid = (int)inc.slot < T->n_used ? T->slot_job[inc.slot] : 0;
+    } else {
+        inc = T->last_incident;  // from a batch already reset
+        jid = T->incident_job;
+    }
+    if (!inc.flag) return OCTMPS_OK;
+    out->stopped = 1;
+    out->job = jid;
+    auto it = ctx->jobs.find(jid);
+    if (it != ctx->jobs.end()) {
+        out->seed = it->second->seed;
+        out->n_lanes = it->second->n_lanes;
+        out->n_photons = it->second->n_photons;
+    }
+    out->lane = inc.lane;
+    out->packets_left = inc.packets_left;
+    out->steps = inc.steps;
+    out->tet = inc.tet;
+    for (int k = 0; k < 3; ++k) {
+        out->pos[k] = inc.pos[k];
+        out->dir[k] = inc.dir[k];
+    }
+    out->weight = inc.w;
+    out->step_left = inc.sleft;
+    return OCTMPS_OK;
+}
+
+// Test hook: per-lane records of the first packets of the most recently
+// submitted job, run by the next launch, which waits for the table's running
+// launches to end first (device buffer of n_lanes records, 80 bytes each).
 octmps_status octmps_debug_record_next_launch(octmps_ctx *ctx, void *device_records) {
     if (!ctx) return OCTMPS_ERR_INVALID_ARG;
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
@@ -615,51 +1060,22 @@ octmps_status octmps_debug_record_next_launch(octmps_ctx *ctx, void *device_reco
 
 octmps_status octmps_job_wait(octmps_ctx *ctx, octmps_job_id id, int32_t timeout_ms) {
     if (!ctx) return OCTMPS_ERR_INVALID_ARG;
-    std::shared_ptr<Launch> L;
-    {
-        std::lock_guard<std::recursive_mutex> g(ctx->mu);
-        cudaSetDevice(ctx->device);
-        auto it = ctx->jobs.find(id);
-        if (it == ctx->jobs.end()) return fail(ctx, OCTMPS_ERR_NOT_FOUND, "unknown job id");
-        Job *j = it->second.get();
-        if (j->done) return j->status;
-        if (!j->launch) {
-            octmps_status st = flush_locked(ctx);
-            if (st != OCTMPS_OK) return st;
-        }
-        L = j->launch;
-    }
     const double t0 = now_ms();
     for (;;) {
-        cudaError_t q;
         {
             std::lock_guard<std::recursive_mutex> g(ctx->mu);
-            if (L->complete) break;
-            q = cudaEventQuery(L->stop);
-            if (q == cudaSuccess) {
-                octmps_status st = finish_launch(ctx, L);
-                if (st != OCTMPS_OK) return st;
-                break;
-            }
-            if (q != cudaErrorNotReady) return cuda_fail(ctx, q, "launch");
+            cudaSetDevice(ctx->device);
+            auto it = ctx->jobs.find(id);
+            if (it == ctx->jobs.end()) return fail(ctx, OCTMPS_ERR_NOT_FOUND, "unknown job id");
+            Job &j = *it->second;
+            octmps_status st = job_check(ctx, j);
+            if (st != OCTMPS_OK) return st;
+            if (j.done) return j.status;
         }
         if (timeout_ms >= 0 && now_ms() - t0 > timeout_ms)
             return fail(ctx, OCTMPS_ERR_TIMEOUT, "job not finished within the timeout");
-        std::this_thread::sleep_for(std::chrono::microseconds(200));
+        std::this_thread::sleep_for(std::chrono::microseconds(100));
     }
-    std::lock_guard<std::recursive_mutex> g(ctx->mu);
-    Job *j = ctx->jobs[id].get();
-    if (!j->done) {
-        j->done = true;
-        j->t_done = now_ms();
-        if (L->error) {
-            j->status = OCTMPS_ERR_KERNEL;
-            char msg[96];
-            snprintf(msg, sizeof msg, "kernel error word 0x%x", L->error);
-            ctx->err = msg;
-        }
-    }
-    return j->status;
 }
 
 octmps_status octmps_job_fetch(octmps_ctx *ctx, octmps_job_id id, octmps_tally *out) {
@@ -719,7 +1135,18 @@ octmps_status octmps_job_fetch_stats(octmps_ctx *ctx, octmps_job_id id, octmps_j
     out->steps = s[0];
     out->restores = s[1];
     out->packets = s[2];
-    out->device_ms = j->launch ? j->launch->ms : 0.0;
+    // device time of the launch the job finished in, once that launch has
+    // ended (a job can finish well before the launch does; this never waits)
+    out->device_ms = -1.0;
+    out->launch_id = 0;
+    if (j->launch) {
+        if (!j->launch->ended && cudaEventQuery(j->launch->stop) == cudaSuccess) {
+            cudaEventElapsedTime(&j->launch->ms, j->launch->start, j->launch->stop);
+            j->launch->ended = true;
+        }
+        if (j->launch->ended) out->device_ms = j->launch->ms;
+        out->launch_id = j->launch->seq;
+    }
     out->submit_to_done_ms = j->t_done - j->t_submit;
     return st;
 }
@@ -730,14 +1157,22 @@ octmps_status octmps_job_release(octmps_ctx *ctx, octmps_job_id id) {
     auto it = ctx->jobs.find(id);
     if (it == ctx->jobs.end()) return OCTMPS_ERR_NOT_FOUND;
     Job *j = it->second.get();
-    if (!j->launch) {
-        // still queued: drop it from the queue
-        ctx->pending.erase(std::remove(ctx->pending.begin(), ctx->pending.end(), id),
-                           ctx->pending.end());
-    } else if (!j->launch->complete) {
-        octmps_status st = finish_launch(ctx, j->launch);
-        if (st != OCTMPS_OK) return st;
+    if (!j->done) {
+        // A job in the table runs to its end (its device buffers are in use);
+        // one still waiting for a slot is simply dropped.
+        Table &T = *ctx->tables[j->precision];
+        auto w = std::find(T.waiting.begin(), T.waiting.end(), id);
+        if (w != T.waiting.end()) {
+            T.waiting.erase(w);
+        } else {
+            octmps_status st = octmps_job_wait(ctx, id, -1);
+            if (st != OCTMPS_OK && st != OCTMPS_ERR_KERNEL) return st;
+        }
     }
+    // The job's buffers may still be named by its table slot until the table
+    // resets, but the kernel no longer touches them once every lane of the
+    // job has reported (its last writes are fenced before the report), so
+    // they are freed without waiting for the launch to end.
     release_job_device(ctx, j);
     ctx->jobs.erase(it);
     return OCTMPS_OK;

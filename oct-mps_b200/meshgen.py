@@ -138,6 +138,93 @@ def config_bscan(out_dir, n_ascans=256, n_photons=1_000_000, nx=64, ny=32, nz=31
                        [TISSUE, (1.40, 0.15, 90.0, 0.9), (1.38, 0.3, 120.0, 0.95)], probe)
 
 
+def layered_grid(nx, ny, h, x0, y0, surfaces, cells_per_layer):
+    """A structured grid whose node z follows the layer surfaces: column
+    (i, j) runs from surface 0 down through each layer, with
+    cells_per_layer[l] cells spaced evenly between surfaces l and l+1, so every
+    interface is a face of the grid.  surfaces[l](X, Y) gives depth.  Regions
+    are the layer numbers (1-based)."""
+    nz = int(sum(cells_per_layer))
+    xs = x0 + h * np.arange(nx + 1)
+    ys = y0 + h * np.arange(ny + 1)
+    X, Y = np.meshgrid(xs, ys, indexing="xy")  # [ny+1, nx+1]
+    Z = np.zeros((nz + 1, ny + 1, nx + 1))
+    layer_of_cell = np.zeros(nz, np.int64)
+    k = 0
+    for l, n in enumerate(cells_per_layer):
+        top, bot = surfaces[l](X, Y), surfaces[l + 1](X, Y)
+        for c in range(n):
+            Z[k + c] = top + (bot - top) * (c / n)
+            layer_of_cell[k + c] = l + 1
+        k += n
+    Z[nz] = surfaces[-1](X, Y)
+    verts = np.stack([np.broadcast_to(X, Z.shape).ravel(), np.broadcast_to(Y, Z.shape).ravel(),
+                      Z.ravel()], axis=1)
+    vid = lambda i, j, kk: (kk * (ny + 1) + j) * (nx + 1) + i  # noqa: E731
+    ck, cj, ci = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    ck, cj, ci = ck.ravel(), cj.ravel(), ci.ravel()
+    tets = np.zeros((len(ck), 6, 5), np.int64)
+    for t, perm in enumerate(PERMS):
+        off = np.zeros(3, int)
+        corners = [vid(ci, cj, ck)]
+        for ax in perm:
+            off[ax] += 1
+            corners.append(vid(ci + off[0], cj + off[1], ck + off[2]))
+        tets[:, t, :4] = np.stack(corners, axis=1) + 1
+        tets[:, t, 4] = layer_of_cell[ck]
+    return verts, tets.reshape(-1, 5)
+
+
+def config_layers(out_dir, n_photons=10_000_000, nx=60, ny=60, nz=46, n_ascans=64):
+    """Config 3, the precision study: a 2 x 2 x 1.5 mm slab of four layers
+    (0.1 / 0.2 / 0.4 / 0.8 mm; mu_s 4 / 10 / 7 / 9 per mm; g 0.9 / 0.95 / 0.9 /
+    0.85; n 1.33 / 1.40 / 1.37 / 1.35; mu_a 0.01 / 0.02 / 0.03 / 0.02 per mm)
+    whose two middle interfaces are tilted 5 degrees about y.  60x60x46 mapped
+    cells (993,600 tets), about 1 um depth bins (Lc = 6 um), 64 A-scans 10 um
+    apart."""
+    h = 0.2 / nx
+    x0 = -0.1 - 0.02 * h
+    y0 = -0.1 - 0.51 * h
+    tilt = np.tan(np.radians(5.0))
+    surfaces = [lambda X, Y: 0.0 * X, lambda X, Y: 0.01 + 0.0 * X,
+                lambda X, Y: 0.03 + tilt * X, lambda X, Y: 0.07 + tilt * X,
+                lambda X, Y: 0.15 + 0.0 * X]
+    thick = np.array([0.01, 0.02, 0.04, 0.08])
+    cells = np.maximum(1, np.round(thick / thick.sum() * nz)).astype(int)
+    cells[-1] += nz - cells.sum()
+    verts, tets = layered_grid(nx, ny, h, x0, y0, surfaces, cells)
+    regions = [(1.33, 0.1, 40.0, 0.9), (1.40, 0.2, 100.0, 0.95), (1.37, 0.3, 70.0, 0.9),
+               (1.35, 0.2, 90.0, 0.85)]
+    start = -0.001 * (n_ascans // 2)
+    probe = (start, 0.001, start + 0.001 * n_ascans - 0.0005)
+    return _write_deck(out_dir, "layers", verts, tets, n_photons, regions, probe, lc=0.0006)
+
+
+def config_random_job(out_dir, rng, index, target_tets=None, n_photons=None):
+    """Config 4, one job of the batched uneven set: the 2 x 2 x 1.5 mm box
+    with 1-4 ellipsoid inclusions (semi-axes 0.1-0.8 mm, mu_s 5-15 per mm, g
+    0.8-0.95, n 1.33-1.45), a grid sized for 50k-800k tets and a log-uniform
+    number of packets in 1e4-1e7."""
+    tets = target_tets or int(10 ** rng.uniform(np.log10(5e4), np.log10(8e5)))
+    n = max(4, int(round((tets / (6 * 0.75)) ** (1 / 3))))
+    nx, ny, nz = n, n, max(3, int(round(0.75 * n)))
+    h = 0.2 / nx
+    x0 = -0.1 - 0.02 * h
+    y0 = -0.1 - 0.51 * h
+    regions = [TISSUE]
+    incl = []
+    for _ in range(int(rng.integers(1, 5))):
+        a = rng.uniform(0.01, 0.08, 3)
+        c = (rng.uniform(-0.06, 0.06), rng.uniform(-0.06, 0.06), rng.uniform(0.03, 0.12))
+        regions.append((float(rng.uniform(1.33, 1.45)), 0.15, float(rng.uniform(50, 150)),
+                        float(rng.uniform(0.8, 0.95))))
+        incl.append(Inclusion(c, a, len(regions)))
+    verts, tets_arr = grid_mesh(nx, ny, nz, h, x0, y0, incl)
+    photons = n_photons or int(10 ** rng.uniform(4, 7))
+    return _write_deck(out_dir, f"job{index}", verts, tets_arr, photons, regions,
+                       (0.0, 0.001, 0.0005))
+
+
 def config_small(out_dir, n_photons=20_000, nx=8, ny=8, nz=6, matched=False):
     """A small deck of the same construction for quick parity checks."""
     h = 0.2 / nx

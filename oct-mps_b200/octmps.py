@@ -105,6 +105,7 @@ class JobStats(C.Structure):
     _fields_ = [
         ("packets", C.c_uint64), ("steps", C.c_uint64), ("restores", C.c_uint64),
         ("device_ms", C.c_double), ("submit_to_done_ms", C.c_double),
+        ("launch_id", C.c_int64),
     ]
 
 
@@ -112,7 +113,16 @@ class LaunchConfig(C.Structure):
     _fields_ = [
         ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("default_lanes", C.c_int32),
         ("use_graphs", C.c_int32), ("hbm_budget_bytes", C.c_uint64),
-        ("scatter_share", C.c_int32),
+        ("scatter_share", C.c_int32), ("linger_us", C.c_int32),
+    ]
+
+
+class Incident(C.Structure):
+    _fields_ = [
+        ("stopped", C.c_int32), ("tet", C.c_int32), ("job", C.c_int64), ("seed", C.c_uint64),
+        ("n_lanes", C.c_uint64), ("n_photons", C.c_uint64), ("lane", C.c_uint64),
+        ("packets_left", C.c_uint64), ("steps", C.c_uint64), ("pos", C.c_double * 3),
+        ("dir", C.c_double * 3), ("weight", C.c_double), ("step_left", C.c_double),
     ]
 
 
@@ -121,7 +131,8 @@ EXPORTED = [
     "octmps_ctx_create", "octmps_ctx_destroy", "octmps_last_error", "octmps_status_string",
     "octmps_ctx_set_multipliers", "octmps_ctx_configure", "octmps_mesh_build_file",
     "octmps_mesh_host_free", "octmps_mesh_find_root", "octmps_mesh_upload", "octmps_mesh_release",
-    "octmps_rng_init", "octmps_job_submit", "octmps_ctx_flush", "octmps_job_wait",
+    "octmps_rng_init", "octmps_job_submit", "octmps_ctx_flush", "octmps_ctx_synchronize",
+    "octmps_ctx_poll", "octmps_debug_incident", "octmps_job_wait",
     "octmps_job_fetch", "octmps_job_fetch_stats", "octmps_job_release", "octmps_read_opt",
     "octmps_read_mci", "octmps_write_result", "octmps_safeprimes_generate",
     "octmps_safeprimes_write", "octmps_safeprimes_read", "octmps_ascan_run_noalloc",
@@ -155,6 +166,9 @@ def lib():
                                           P(RngLanes)]),
             "octmps_job_submit": (C.c_int, [C.c_void_p, P(Job), P(C.c_int64)]),
             "octmps_ctx_flush": (C.c_int, [C.c_void_p]),
+            "octmps_ctx_synchronize": (C.c_int, [C.c_void_p]),
+            "octmps_ctx_poll": (C.c_int, [C.c_void_p, P(C.c_int64), C.c_int32, P(C.c_int32)]),
+            "octmps_debug_incident": (C.c_int, [C.c_void_p, C.c_int32, P(Incident)]),
             "octmps_job_wait": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32]),
             "octmps_job_fetch": (C.c_int, [C.c_void_p, C.c_int64, P(Tally)]),
             "octmps_job_fetch_stats": (C.c_int, [C.c_void_p, C.c_int64, P(JobStats)]),
@@ -352,8 +366,10 @@ class Context:
         a = np.ascontiguousarray(a, dtype=np.uint32)
         _check(lib().octmps_ctx_set_multipliers(self.h, _ptr(a, C.c_uint32), len(a)), self.h)
 
-    def configure(self, blocks_per_sm=0, default_lanes=0, hbm_budget_bytes=0, scatter_share=0):
-        cfg = LaunchConfig(0, blocks_per_sm, default_lanes, 0, hbm_budget_bytes, scatter_share)
+    def configure(self, blocks_per_sm=0, default_lanes=0, hbm_budget_bytes=0, scatter_share=0,
+                  linger_us=0):
+        cfg = LaunchConfig(0, blocks_per_sm, default_lanes, 0, hbm_budget_bytes, scatter_share,
+                           linger_us)
         _check(lib().octmps_ctx_configure(self.h, C.byref(cfg)), self.h)
 
     def upload_mesh(self, mesh):
@@ -382,6 +398,30 @@ class Context:
     def flush(self):
         _check(lib().octmps_ctx_flush(self.h), self.h)
 
+    def last_error(self):
+        return lib().octmps_last_error(self.h).decode()
+
+    def synchronize(self):
+        """Waits until every launch of the context has ended."""
+        _check(lib().octmps_ctx_synchronize(self.h), self.h)
+
+    def poll(self, max_ids=1024):
+        """Ids of jobs finished since the last poll (never waits)."""
+        buf = (C.c_int64 * max_ids)()
+        n = C.c_int32()
+        _check(lib().octmps_ctx_poll(self.h, buf, max_ids, C.byref(n)), self.h)
+        return list(buf[: n.value])
+
+    def incident(self, precision=PREC_MIXED):
+        """The first packet of the precision's job table stopped at the step
+        cap (None if none), as a dict."""
+        inc = Incident()
+        _check(lib().octmps_debug_incident(self.h, precision, C.byref(inc)), self.h)
+        if not inc.stopped:
+            return None
+        return {f: (list(getattr(inc, f)) if f in ("pos", "dir") else getattr(inc, f))
+                for f, _ in Incident._fields_}
+
     def wait(self, jid, timeout_ms=-1):
         return lib().octmps_job_wait(self.h, jid, timeout_ms)
 
@@ -400,7 +440,8 @@ class Context:
         if st not in (0, 9):
             _check(st, self.h)
         return {"packets": s.packets, "steps": s.steps, "restores": s.restores,
-                "device_ms": s.device_ms, "submit_to_done_ms": s.submit_to_done_ms}
+                "device_ms": s.device_ms, "submit_to_done_ms": s.submit_to_done_ms,
+                "launch_id": s.launch_id}
 
     def release(self, jid):
         _check(lib().octmps_job_release(self.h, jid), self.h)

@@ -231,3 +231,90 @@ def test_cli_end_to_end(octmps, oracle, small_deck, multipliers, tmp_path):
         np.testing.assert_array_equal(got[:, [0, 1, 4]], want[:, [0, 1, 4]])
         np.testing.assert_allclose(got[:, 2:4], want[:, 2:4], rtol=2e-5, atol=0)
     assert (tmp_path / "BiasParam.mco").read_text() == (d / "BiasParam.mco").read_text()
+
+
+def test_jobs_join_a_running_launch_and_match_alone(ctx, octmps, small_deck, small_matched_deck):
+    """Continuous batching: jobs submitted while a long job runs are taken up
+    at once (they finish while it still runs, by the running launch's threads
+    or by a launch started beside it) and give the same counts as each job
+    run alone."""
+    nb = small_deck["sim"].num_optical_depth_length_steps
+    m1 = ctx.upload_mesh(small_deck["mesh"])
+    m2 = ctx.upload_mesh(small_matched_deck["mesh"])
+    late = [(small_matched_deck, m2, 7, 4000, 500), (small_deck, m1, 8, 3000, 300),
+            (small_deck, m1, 9, 2000, 2000)]
+    alone = []
+    for d, mid, seed, n, lanes in late:
+        j = ctx.submit(mid, d["sim"], 0.0, d["root"], n_photons=n, seed=seed, n_lanes=lanes)
+        alone.append(ctx.fetch(j, nb))
+        ctx.release(j)
+    # a long job first (500 packets in a row on each of its 2000 lanes, a
+    # few seconds), then the others while it runs
+    big = ctx.submit(m1, small_deck["sim"], 0.0, small_deck["root"], n_photons=1_000_000,
+                     seed=1, n_lanes=2000)
+    ctx.flush()
+    ids = [ctx.submit(mid, d["sim"], 0.0, d["root"], n_photons=n, seed=seed, n_lanes=lanes)
+           for d, mid, seed, n, lanes in late]
+    ctx.flush()
+    for j, a in zip(ids, alone):
+        b = ctx.fetch(j, nb)
+        assert_tallies_equal(b, a, 0, nb)
+    assert ctx.wait(big, 0) == 4  # the long job still runs (OCTMPS_ERR_TIMEOUT)
+    ctx.fetch(big, nb)
+    assert ctx.stats(big)["packets"] == 1_000_000
+    ctx.synchronize()
+    for j in ids + [big]:
+        s = ctx.stats(j)
+        assert s["launch_id"] >= 1 and s["device_ms"] > 0
+    for j in ids + [big]:
+        ctx.release(j)
+    ctx.release_mesh(m1)
+    ctx.release_mesh(m2)
+
+
+def test_completion_queue_reports_each_job_once(ctx, octmps, small_deck):
+    sim = small_deck["sim"]
+    mid = ctx.upload_mesh(small_deck["mesh"])
+    ids = [ctx.submit(mid, sim, 0.0, small_deck["root"], n_photons=3000 + 100 * k, seed=20 + k,
+                      n_lanes=300) for k in range(5)]
+    ctx.flush()
+    seen = []
+    for _ in range(200000):
+        seen += ctx.poll()
+        if len(seen) >= len(ids):
+            break
+    assert sorted(seen) == sorted(ids)
+    assert ctx.poll() == []
+    for j in ids:
+        assert ctx.wait(j, 0) == 0
+        ctx.release(j)
+    ctx.release_mesh(mid)
+
+
+def test_admission_by_hbm_budget(octmps, multipliers, small_deck, torch_cuda):
+    """Jobs beyond the HBM budget are refused (OCTMPS_ERR_BUDGET) until
+    finished jobs are released."""
+    sim = small_deck["sim"]
+    with octmps.Context(0, multipliers) as c:
+        lanes = 1000
+        nb = sim.num_optical_depth_length_steps
+        # tally block (as laid out on the device) + statistics words, FP64 sums
+        per_job = 32 + 2 * (((nb + 1) * 8 + 15) // 16 * 16) + \
+            6 * (((nb + 2) * 8 + 15) // 16 * 16) + 32
+        c.configure(hbm_budget_bytes=lanes * 36 + 2 * per_job + per_job // 2)
+        mid = c.upload_mesh(small_deck["mesh"])
+        a = c.submit(mid, sim, 0.0, small_deck["root"], n_photons=2000, seed=3, n_lanes=lanes)
+        b = c.submit(mid, sim, 0.0, small_deck["root"], n_photons=2000, seed=3, n_lanes=lanes)
+        with pytest.raises(octmps.OctmpsError) as e:
+            c.submit(mid, sim, 0.0, small_deck["root"], n_photons=2000, seed=3, n_lanes=lanes)
+        assert e.value.status == 8
+        c.flush()
+        c.fetch(a, nb)
+        c.release(a)
+        c.synchronize()  # released memory counts until no launch runs
+        d = c.submit(mid, sim, 0.0, small_deck["root"], n_photons=2000, seed=3, n_lanes=lanes)
+        c.flush()
+        for j in (b, d):
+            c.fetch(j, nb)
+            c.release(j)
+        c.release_mesh(mid)
