@@ -169,6 +169,9 @@ typedef struct {
                              while that launch still runs (never waits) */
     double submit_to_done_ms;
     int64_t launch_id;    /* sequence number (per context) of that launch */
+    uint64_t stopped;     /* packets stopped: at the step cap (2^26 steps, an error) or
+                             after 1000 boundary hits in a row that did not move the
+                             photon (a packet the reference would run forever) */
 } octmps_job_stats;
 
 /* ---- context ------------------------------------------------------------ */
@@ -238,12 +241,11 @@ octmps_status octmps_job_fetch_stats(octmps_ctx *ctx, octmps_job_id id, octmps_j
 octmps_status octmps_job_release(octmps_ctx *ctx, octmps_job_id id);
 
 /* Diagnosis: the first packet of a precision's job table (its current batch,
- * else the latest batch that had one) that was stopped at the step cap (2^26
- * steps; the reference has no cap), with the state it was stopped in; seed,
- * n_lanes and n_photons are filled while the job is not released.
- * stopped = 0 if none. */
+ * else the latest batch that had one) that was stopped, with the state it
+ * was stopped in; seed, n_lanes and n_photons are filled while the job is
+ * not released. */
 typedef struct {
-    int32_t stopped;
+    int32_t stopped;        /* 0 none, 1 step cap, 2 no progress */
     int32_t tet;
     octmps_job_id job;
     uint64_t seed, n_lanes, n_photons;

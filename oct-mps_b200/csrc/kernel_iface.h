@@ -90,8 +90,8 @@ OCTMPS_HD inline TallyLayout tally_layout(int nbins, size_t psize) {
     return L;
 }
 
-// The first packet a table's launches stopped at the step cap, for
-// diagnosis (written once; cleared when the table is reset).
+// The first packet a table's launches stopped (flag 1: step cap; 2: no
+// progress), for diagnosis; written once, cleared when the table is reset.
 struct Incident {
     unsigned int flag;
     unsigned int slot;

@@ -93,6 +93,7 @@ __device__ __forceinline__ unsigned long long fnv(unsigned long long h, unsigned
     return h;
 }
 
+constexpr uint32_t kStallHits = 1000;    // see the stop rule in the kernel loop
 constexpr uint32_t kRetryUs = 8;         // first retry interval of a thread waiting for work
 constexpr uint32_t kRetryMaxUs = 512;    // the interval doubles up to this
 constexpr unsigned kIdleSleepNs = 4000;  // pause of a warp whose lanes all wait
@@ -221,6 +222,7 @@ struct Lane {
         fst_flag = 0;
         loc_fst = -1;
         num_back = 0;
+        stall = 0;
         tet = jd->root_tet;
         if (jd->root_region != region) load_region(jd->root_region);
         if (kRecord) {
@@ -484,6 +486,7 @@ struct Lane {
             sleft = (s - min_d) * rg.muas;
             s = min_d;
         }
+        stall = (hit && s <= (T)0) ? stall + 1 : 0;
         // Hop, :574-582
         x = DevNum<T>::mad(s, ux, x);
         y = DevNum<T>::mad(s, uy, y);
@@ -630,6 +633,7 @@ struct Lane {
                 ev |= 32;
                 if (kRecord) ++rrestores;
                 restores_++;
+                stall = 0;
             } else {
                 ev |= 64;
                 end = true;
@@ -642,6 +646,7 @@ struct Lane {
         return end;
     }
     uint32_t restores_;
+    uint32_t stall;  // consecutive boundary hits that did not move the photon
 };
 
 // kMinBlocks: resident blocks per SM the register allocation must allow
@@ -803,12 +808,23 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
         }
         ++steps_packet;
         bool done = end;
+        // A packet is stopped (its split copy too) at the step cap, an
+        // error, or after kStallHits boundary hits in a row that did not
+        // move it: a photon on a face moving parallel to it (the cosine of
+        // incidence below the grazing limit) is reflected with its direction
+        // unchanged, the same hit again at distance 0, forever.
+        unsigned reason = 0;
         if (!done && steps_packet >= args.step_cap) {
             atomicOr(err, kErrStepCap);
+            reason = 1;
+        } else if (!done && L.stall >= kStallHits) {
+            reason = 2;
+        }
+        if (reason) {
             atomicAdd(&L.jd->stats[3], 1ull);
             done = true;
             Incident *inc = args.incident;
-            if (inc && atomicCAS(&inc->flag, 0u, 1u) == 0u) {
+            if (inc && atomicCAS(&inc->flag, 0u, reason) == 0u) {
                 inc->slot = (unsigned)slot;
                 inc->tet = L.tet;
                 inc->packets_left = packets_left;

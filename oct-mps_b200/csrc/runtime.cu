@@ -1027,7 +1027,7 @@ octmps_status octmps_debug_incident(octmps_ctx *ctx, int32_t precision, octmps_i
         jid = T->incident_job;
     }
     if (!inc.flag) return OCTMPS_OK;
-    out->stopped = 1;
+    out->stopped = (int32_t)inc.flag;
     out->job = jid;
     auto it = ctx->jobs.find(jid);
     if (it != ctx->jobs.end()) {
@@ -1135,6 +1135,7 @@ octmps_status octmps_job_fetch_stats(octmps_ctx *ctx, octmps_job_id id, octmps_j
     out->steps = s[0];
     out->restores = s[1];
     out->packets = s[2];
+    out->stopped = s[3];
     // device time of the launch the job finished in, once that launch has
     // ended (a job can finish well before the launch does; this never waits)
     out->device_ms = -1.0;

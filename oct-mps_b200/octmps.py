@@ -105,7 +105,7 @@ class JobStats(C.Structure):
     _fields_ = [
         ("packets", C.c_uint64), ("steps", C.c_uint64), ("restores", C.c_uint64),
         ("device_ms", C.c_double), ("submit_to_done_ms", C.c_double),
-        ("launch_id", C.c_int64),
+        ("launch_id", C.c_int64), ("stopped", C.c_uint64),
     ]
 
 
@@ -441,7 +441,7 @@ class Context:
             _check(st, self.h)
         return {"packets": s.packets, "steps": s.steps, "restores": s.restores,
                 "device_ms": s.device_ms, "submit_to_done_ms": s.submit_to_done_ms,
-                "launch_id": s.launch_id}
+                "launch_id": s.launch_id, "stopped": s.stopped}
 
     def release(self, jid):
         _check(lib().octmps_job_release(self.h, jid), self.h)

@@ -699,7 +699,9 @@ struct Lane {
     // (OCTMPSKernel loop body, src/octmps_kernel.cuh:1349-1392).
     void run(uint64_t packets, OraclePacket *first_rec) {
         Photon<T, P> ph, cont;
-        const uint64_t cap = 1ull << 34;
+        // steps allowed per packet, as the kernel's step_cap; a dump ends
+        // its packet at the dump's length
+        const uint64_t cap = dump ? (uint64_t)dump_max : (1ull << 26);
         for (uint64_t k = 0; k < packets; ++k) {
             rec = (k == 0) ? first_rec : nullptr;
             rec_contrib = 0;
@@ -709,10 +711,12 @@ struct Lane {
             cont = ph;
             tally.packets++;
             uint64_t steps = 0;
+            uint32_t stall = 0;  // boundary hits in a row that did not move the photon
             for (;;) {
                 int ev;
                 step_size(ph);
                 const bool hit = hit_boundary(ph);
+                stall = (hit && ph.s <= (T)0) ? stall + 1 : 0;
                 hop(ph);
                 if (hit) {
                     ev = reflect_transmit(ph);
@@ -741,6 +745,7 @@ struct Lane {
                         spin(S.regions[S.region[ph.tet]].g, ph);
                         ph.lr = lr_tmp < (T)1 ? (T)1 - lr_tmp : (T)1;
                         ev |= ORACLE_EV_RESTORE;
+                        stall = 0;
                         r.restores++;
                         tally.restores++;
                     } else {
@@ -758,7 +763,12 @@ struct Lane {
                 r.steps++;
                 ++steps;
                 if (end) break;
-                if (steps >= cap) {
+                // The kernel's stop rule: the step cap, or 1000 hits in a row
+                // that did not move the photon (a photon on a face moving
+                // parallel to it is reflected with its direction unchanged
+                // by the grazing-incidence rule, again at distance 0; the
+                // reference repeats that forever).
+                if (steps >= cap || stall >= 1000) {
                     tally.capped++;
                     break;
                 }

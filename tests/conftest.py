@@ -98,3 +98,21 @@ def three_sigma_ok(sum_a, sumsq_a, n_a, sum_b, sumsq_b, n_b, k=3.0, min_count=No
     if len(z) == 0:
         return 1.0, 0.0
     return float(np.mean(z <= k)), float(np.max(z))
+
+
+@pytest.fixture(scope="session")
+def plain_2m_deck(octmps, meshgen, workdir):
+    """The plain A-scan geometry on a 70 x 70 x 68 grid (1,999,200 tets)."""
+    p = meshgen.config_plain_ascan(os.path.join(workdir, "plain2m"), nx=70, ny=70, nz=68)
+    sim = octmps.read_deck(p["opt"], p["mci"])
+    mesh = octmps.build_mesh(p["mesh"])
+    return {"paths": p, "sim": sim, "mesh": mesh}
+
+
+# A packet that makes no progress: on plain_2m_deck, probe x below, seed
+# 2074, RNG lane 5618's first packet ends on a diagonal face of the grid,
+# on a vertical grid edge, moving parallel to the face (ux == uy); the
+# grazing-incidence rule reflects it there with its direction unchanged, at
+# distance 0, again and again.  The stop rule ends it after 1000 such hits
+# (step 6502).
+STUCK_CASE = {"x": 0.0051907104324341955, "seed": 2074, "lane": 5618, "steps": 6502}

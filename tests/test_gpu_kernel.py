@@ -318,3 +318,23 @@ def test_admission_by_hbm_budget(octmps, multipliers, small_deck, torch_cuda):
             c.fetch(j, nb)
             c.release(j)
         c.release_mesh(mid)
+
+
+def test_stopped_packet_bit_exact_on_2m_tet_mesh(ctx, torch_cuda, octmps, oracle, multipliers,
+                                                  plain_2m_deck):
+    """First packets of 5619 lanes on the 1,999,200-tet mesh, the last of them
+    a packet that makes no progress: the kernel stops it at the same step as
+    the oracle (one stopped packet), and every record and count agrees."""
+    from conftest import STUCK_CASE as S
+    d = dict(plain_2m_deck)
+    d["root"] = d["mesh"].find_root(S["x"])
+    d["sim"] = type(d["sim"]).from_buffer_copy(d["sim"])  # probe at the case's x
+    d["sim"].start_x = S["x"]
+    lanes = S["lane"] + 1
+    t_g, st, r_g = run_gpu(ctx, torch_cuda, d, lanes, lanes, S["seed"], 0)
+    t_o, r_o = run_oracle(oracle, octmps, d, lanes, lanes, S["seed"], 0, multipliers)
+    assert st["stopped"] == 1 and t_o["capped"] == 1
+    assert r_g["steps"][S["lane"]] == S["steps"]
+    assert st["steps"] == t_o["steps"]
+    assert_records_equal(r_g, r_o)
+    assert_tallies_equal(t_g, t_o, 0, d["sim"].num_optical_depth_length_steps)

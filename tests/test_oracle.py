@@ -158,3 +158,16 @@ def test_oracle_is_deterministic(oracle, octmps, small_deck):
                    rng, 0, n_threads=3)
     for k in a:
         np.testing.assert_array_equal(a[k], b[k])
+
+
+def test_oracle_stops_a_packet_that_makes_no_progress(octmps, oracle, multipliers, plain_2m_deck):
+    from conftest import STUCK_CASE as S
+    import oracle_py
+    d = plain_2m_deck
+    root = d["mesh"].find_root(S["x"])
+    rng = octmps.rng_init(multipliers[: 3 + 3 * (S["lane"] + 1)], S["lane"] + 1, S["seed"])
+    one = {k: v[S["lane"]:S["lane"] + 1].copy() for k, v in rng.items()}
+    t, rec = oracle.run(oracle_py.params_from_sim(d["sim"]), d["mesh"], (S["x"], 0.0, 0.0), root,
+                        1, 1, one, 0, record=True)
+    assert t["capped"] == 1
+    assert rec["steps"][0] == S["steps"]
