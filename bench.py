@@ -217,6 +217,32 @@ def run_ours(args, rank, world, local_rank, dist):
     barrier()
     clocks = sampler.stop()
 
+    # The same workload one A-scan per launch (submit, run, fetch, next), on
+    # the first A-scans of the scan: the batched launches' gain over the
+    # plain single-job use.  Compared in propagation steps per second (the
+    # A-scans differ in steps per packet).  Untimed for the headline.
+    ctx.configure(linger_us=-1)
+    plain_ms, plain_steps, plain_packets = 0.0, 0, 0
+    for k in range(min(args.plain_ascans, len(xs))):
+        j = ctx.submit(mid, sim, xs[k], roots[k], n_photons=args.photons, seed=rank * len(xs) + k + 1,
+                       n_lanes=lanes, precision=args.precision)
+        ctx.flush()
+        ctx.fetch(j, nb)
+        ctx.synchronize()
+        s = ctx.stats(j)
+        plain_ms += s["device_ms"]
+        plain_steps += s["steps"]
+        plain_packets += s["packets"]
+        ctx.release(j)
+    ctx.configure(linger_us=0)
+    plain = None
+    if plain_ms > 0:
+        batched_sps = steps / (dev_ms / 1e3)
+        plain_sps = plain_steps / (plain_ms / 1e3)
+        plain = {"ascans": min(args.plain_ascans, len(xs)), "packets_per_s": plain_packets / (plain_ms / 1e3),
+                 "propagation_steps_per_s": plain_sps, "batched_over_plain": batched_sps / plain_sps,
+                 "note": "one A-scan per launch, device time; ratio of propagation steps/s"}
+
     t_dev = torch.tensor([dev_ms, e2e_ms / e2e_steps], dtype=torch.float64, device="cuda")
     if dist is not None:
         dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
@@ -275,6 +301,7 @@ def run_ours(args, rank, world, local_rank, dist):
                              f"({mesh.n_tets * 80 / 1e6:.0f} MB) is L2-resident, the kernel is "
                              f"bound by instruction issue and gather latency"},
         "clocks": clocks,
+        "plain_single_job": plain,
     }
 
 
@@ -356,6 +383,8 @@ def main():
     ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--lanes", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-ascans", type=int, default=4,
+                    help="A-scans run one per launch for the batched-over-plain ratio")
     args = ap.parse_args()
     rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
     local_rank = env_int("LOCAL_RANK", 0)

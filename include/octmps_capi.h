@@ -158,6 +158,8 @@ typedef struct {
     double *sum2;     /* [nbins+2] ReflectanceClassII_Sum */
     double *max2;     /* [nbins+2] */
     double *sumsq2;   /* [nbins+2] */
+    uint64_t num_nonfinite; /* detections whose contribution was NaN or infinite (added
+                               to the sums like any other); filled by octmps_job_fetch */
 } octmps_tally;
 
 /* Per-job statistics filled by octmps_job_fetch_stats. */

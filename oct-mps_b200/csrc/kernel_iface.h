@@ -56,7 +56,8 @@ struct alignas(256) JobDesc {
 static_assert(sizeof(JobDesc) == 256, "a job slot is two cache lines");
 
 // Tally block of one job (P = double or float):
-//   uint64 totals[4]     NumFilteredPhotons, ...ClassI, ...ClassII, pad
+//   uint64 totals[4]     NumFilteredPhotons, ...ClassI, ...ClassII, and the
+//                        number of NaN or infinite contributions added
 //   uint64 count1[nb+1], count2[nb+1]
 //   P      sum1[nb+2], sumsq1[nb+2], sum2[nb+2], sumsq2[nb+2]
 //   P      max1[nb+2], max2[nb+2]  (kept as unsigned bit patterns: the

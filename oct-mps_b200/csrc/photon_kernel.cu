@@ -248,6 +248,10 @@ struct Lane {
         const bool class1 = (P)max_depth > depth - (P)J.half_lc;
         const T c = w * ((T)1 - r_fresnel) * lr;
         const P cp = (P)c;
+        // NaN or infinite: counted, and added like any other.  (Flagging the
+        // lane here instead, through a member of this out-of-line function's
+        // object, halved the kernel's speed.)
+        if (!(cp - cp == (P)0)) atomicAdd(&totals[3], 1ull);
         unsigned long long *cnt =
             reinterpret_cast<unsigned long long *>(base + (class1 ? L.count1 : L.count2));
         P *sum = reinterpret_cast<P *>(base + (class1 ? L.sum1 : L.sum2));
@@ -393,8 +397,16 @@ struct Lane {
         cost = fminT(cost, (T)1);
         rotate(cost, ax, ay, az, true);
 
-        const T costg = dot3<T>(ox, oy, oz, ux, uy, uz);
-        const T costg1 = dot3<T>(vx, vy, vz, ux, uy, uz);
+        T costg = dot3<T>(ox, oy, oz, ux, uy, uz);
+        T costg1 = dot3<T>(vx, vy, vz, ux, uy, uz);
+        if (kFused<T>) {
+            // FP32 forms: a direction rotated about a nearly vertical axis is
+            // off unit length by a few tenths of a percent (1 - uz*uz
+            // cancels), so a cosine can exceed 1 and 1 + g*g - 2*g*cos go
+            // negative under the square root (a NaN likelihood): clamp.
+            costg = fminT(fmaxT(costg, (T)-1), (T)1);
+            costg1 = fminT(fmaxT(costg1, (T)-1), (T)1);
+        }
         if (btmp != (T)0) {
             const T opa2 = DevNum<T>::mad(btmp, btmp, (T)1);
             const T sq_opa2 = sqrtT(opa2);
@@ -823,6 +835,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
         if (reason) {
             atomicAdd(&L.jd->stats[3], 1ull);
             done = true;
+        }
+        if (reason) {
             Incident *inc = args.incident;
             if (inc && atomicCAS(&inc->flag, 0u, reason) == 0u) {
                 inc->slot = (unsigned)slot;

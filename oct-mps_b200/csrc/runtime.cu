@@ -1096,6 +1096,7 @@ octmps_status octmps_job_fetch(octmps_ctx *ctx, octmps_job_id id, octmps_tally *
     out->num_filtered = tot[0];
     out->num_filtered_class1 = tot[1];
     out->num_filtered_class2 = tot[2];
+    out->num_nonfinite = tot[3];
     auto copy_u = [&](uint64_t *dst, size_t off) {
         if (dst) memcpy(dst, h.data() + off, (nb + 1) * sizeof(uint64_t));
     };

@@ -97,7 +97,7 @@ class Tally(C.Structure):
         ("sum1", C.POINTER(C.c_double)), ("max1", C.POINTER(C.c_double)),
         ("sumsq1", C.POINTER(C.c_double)),
         ("sum2", C.POINTER(C.c_double)), ("max2", C.POINTER(C.c_double)),
-        ("sumsq2", C.POINTER(C.c_double)),
+        ("sumsq2", C.POINTER(C.c_double)), ("num_nonfinite", C.c_uint64),
     ]
 
 
@@ -432,6 +432,7 @@ class Context:
         t["num_filtered"] = s.num_filtered
         t["num_filtered_class1"] = s.num_filtered_class1
         t["num_filtered_class2"] = s.num_filtered_class2
+        t["num_nonfinite"] = s.num_nonfinite
         return t
 
     def stats(self, jid):

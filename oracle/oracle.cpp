@@ -313,8 +313,10 @@ struct Lane {
     uint32_t a, aR, aS;
     OraclePacket *rec;  // non-null while recording a packet
     double rec_contrib;
-    double *dump = nullptr;  // per-step state of the first packet (diagnostics)
+    double *dump = nullptr;  // per-step state of packet dump_packet (diagnostics)
     uint32_t dump_max = 0;
+    uint64_t dump_packet = 0;
+    uint64_t dump_rows = 0;
 
     const T *plane(int tet, int k) const { return &S.planes[(size_t)(4 * tet + k) * 4]; }
 
@@ -665,8 +667,16 @@ struct Lane {
         cost = std::fmin(cost, (T)1);
         rotate(cost, ux, uy, uz, ph, true);
 
-        const T costg = dot3<T>(ox, oy, oz, ph.ux, ph.uy, ph.uz);
-        const T costg1 = dot3<T>(vx, vy, vz, ph.ux, ph.uy, ph.uz);
+        T costg = dot3<T>(ox, oy, oz, ph.ux, ph.uy, ph.uz);
+        T costg1 = dot3<T>(vx, vy, vz, ph.ux, ph.uy, ph.uz);
+        if (kFused<T>) {
+            // FP32 forms, as the kernel: a direction rotated about a nearly
+            // vertical axis is off unit length by a few tenths of a percent,
+            // so a cosine can exceed 1 and the likelihood's square root turn
+            // NaN: clamp to [-1, 1]
+            costg = std::fmin(std::fmax(costg, (T)-1), (T)1);
+            costg1 = std::fmin(std::fmax(costg1, (T)-1), (T)1);
+        }
         if (btmp != (T)0) {
             const T opa2 = Num<T>::mad(btmp, btmp, (T)1);
             const T sq_opa2 = std::sqrt(opa2);
@@ -701,7 +711,7 @@ struct Lane {
         Photon<T, P> ph, cont;
         // steps allowed per packet, as the kernel's step_cap; a dump ends
         // its packet at the dump's length
-        const uint64_t cap = dump ? (uint64_t)dump_max : (1ull << 26);
+        const uint64_t cap = (1ull << 26);
         for (uint64_t k = 0; k < packets; ++k) {
             rec = (k == 0) ? first_rec : nullptr;
             rec_contrib = 0;
@@ -754,7 +764,8 @@ struct Lane {
                     }
                 }
                 r.hash = fnv(r.hash, ((uint64_t)(uint32_t)ph.tet << 8) | (uint64_t)ev);
-                if (dump && k == 0 && r.steps < dump_max) {
+                if (dump && k == dump_packet && r.steps < dump_max) {
+                    dump_rows = r.steps + 1;
                     double *d = dump + 12 * (size_t)r.steps;
                     d[0] = ph.tet; d[1] = ev; d[2] = ph.x; d[3] = ph.y; d[4] = ph.z;
                     d[5] = ph.ux; d[6] = ph.uy; d[7] = ph.uz; d[8] = ph.w;
@@ -768,7 +779,8 @@ struct Lane {
                 // parallel to it is reflected with its direction unchanged
                 // by the grazing-incidence rule, again at distance 0; the
                 // reference repeats that forever).
-                if (steps >= cap || stall >= 1000) {
+                if (steps >= cap || stall >= 1000 ||
+                    (dump && k == dump_packet && steps >= dump_max)) {
                     tally.capped++;
                     break;
                 }
@@ -901,7 +913,7 @@ int run_typed(const OracleParams *p, const OracleMesh *m, double px, double py, 
 template <typename T, typename P>
 int dump_typed(const OracleParams *p, const OracleMesh *m, double px, double py, double pz,
                int32_t root, uint64_t x, uint32_t a, uint64_t xR, uint32_t aR, uint64_t xS,
-               uint32_t aS, double *out, uint32_t max_steps) {
+               uint32_t aS, double *out, uint32_t max_steps, uint64_t packet_index) {
     Setup<T, P> S;
     make_setup(S, p, m, px, py, pz, root);
     Tally<T, P> tl(p->nbins);
@@ -909,8 +921,9 @@ int dump_typed(const OracleParams *p, const OracleMesh *m, double px, double py,
     Lane<T, P> L{S, tl, x, xR, xS, a, aR, aS, nullptr, 0.0};
     L.dump = out;
     L.dump_max = max_steps;
-    L.run(1, &rec);
-    return (int)rec.steps;
+    L.dump_packet = packet_index;
+    L.run(packet_index + 1, &rec);
+    return (int)L.dump_rows;
 }
 
 }  // namespace
@@ -943,17 +956,17 @@ int oracle_run(const OracleParams *p, const OracleMesh *m, double probe_x, doubl
 int oracle_dump_lane(const OracleParams *p, const OracleMesh *m, double probe_x, double probe_y,
                      double probe_z, int32_t root, uint64_t x, uint32_t a, uint64_t xR,
                      uint32_t aR, uint64_t xS, uint32_t aS, int precision, double *out,
-                     uint32_t max_steps) {
+                     uint32_t max_steps, uint64_t packet_index) {
     switch (precision) {
         case 0:
             return dump_typed<float, double>(p, m, probe_x, probe_y, probe_z, root, x, a, xR, aR,
-                                             xS, aS, out, max_steps);
+                                             xS, aS, out, max_steps, packet_index);
         case 1:
             return dump_typed<float, float>(p, m, probe_x, probe_y, probe_z, root, x, a, xR, aR,
-                                            xS, aS, out, max_steps);
+                                            xS, aS, out, max_steps, packet_index);
         case 2:
             return dump_typed<double, double>(p, m, probe_x, probe_y, probe_z, root, x, a, xR, aR,
-                                              xS, aS, out, max_steps);
+                                              xS, aS, out, max_steps, packet_index);
     }
     return -1;
 }

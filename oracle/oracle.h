@@ -102,13 +102,14 @@ int oracle_run(const OracleParams *p, const OracleMesh *m, double probe_x, doubl
                const uint64_t *xS, const uint32_t *aS, int precision, int n_threads,
                OracleTally *out, OraclePacket *first);
 
-/* Per-step state of one lane's first packet (diagnostics of the first
- * divergence against the reference): per step 12 doubles
- * tet, event, x, y, z, ux, uy, uz, w, s, optical path, likelihood ratio. */
+/* Per-step state of one lane's packet number packet_index (0 = its first;
+ * diagnostics): per step 12 doubles tet, event, x, y, z, ux, uy, uz, w, s,
+ * optical path, likelihood ratio; at most max_steps steps (the dumped packet
+ * ends there).  Returns the number of steps written. */
 int oracle_dump_lane(const OracleParams *p, const OracleMesh *m, double probe_x, double probe_y,
                      double probe_z, int32_t root, uint64_t x, uint32_t a, uint64_t xR,
                      uint32_t aR, uint64_t xS, uint32_t aS, int precision, double *out,
-                     uint32_t max_steps);
+                     uint32_t max_steps, uint64_t packet_index);
 
 /* The math kernels of the method, exposed for unit tests. */
 float oracle_logf(float x);

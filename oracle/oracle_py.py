@@ -150,7 +150,7 @@ class Oracle:
         L.oracle_dump_lane.argtypes = [P(OracleParams), P(OracleMesh), C.c_double, C.c_double,
                                        C.c_double, C.c_int32, C.c_uint64, C.c_uint32,
                                        C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, C.c_int,
-                                       P(C.c_double), C.c_uint32]
+                                       P(C.c_double), C.c_uint32, C.c_uint64]
         L.oracle_logf.restype = C.c_float
         L.oracle_logf.argtypes = [C.c_float]
         L.oracle_log.restype = C.c_double
@@ -175,14 +175,16 @@ class Oracle:
         m.planes = _ptr(mesh.planes, C.c_double)
         return m
 
-    def dump_lane(self, params, mesh, probe, root, rng, lane, precision, max_steps=100000):
-        """Per-step state (tet, event, x, y, z, ux, uy, uz, w, s, path, LR) of a lane's first packet."""
+    def dump_lane(self, params, mesh, probe, root, rng, lane, precision, max_steps=100000,
+                  packet=0):
+        """Per-step state (tet, event, x, y, z, ux, uy, uz, w, s, path, LR) of a lane's
+        packet number `packet` (0 = first)."""
         out = np.zeros((max_steps, 12))
         n = self.L.oracle_dump_lane(C.byref(params), C.byref(self._mesh(mesh)), probe[0], probe[1],
                                     probe[2], root, int(rng["x"][lane]), int(rng["a"][lane]),
                                     int(rng["xR"][lane]), int(rng["aR"][lane]),
                                     int(rng["xS"][lane]), int(rng["aS"][lane]), precision,
-                                    _ptr(out, C.c_double), max_steps)
+                                    _ptr(out, C.c_double), max_steps, packet)
         return out[:min(n, max_steps)]
 
     def run(self, params, mesh, probe, root, n_photons, n_lanes, rng, precision, n_threads=0,

@@ -116,3 +116,22 @@ def plain_2m_deck(octmps, meshgen, workdir):
 # distance 0, again and again.  The stop rule ends it after 1000 such hits
 # (step 6502).
 STUCK_CASE = {"x": 0.0051907104324341955, "seed": 2074, "lane": 5618, "steps": 6502}
+
+
+@pytest.fixture(scope="session")
+def layers_deck(octmps, meshgen, workdir):
+    """The four-layer slab with tilted interfaces (993,600 tets, 1499 bins)."""
+    p = meshgen.config_layers(os.path.join(workdir, "layers"))
+    sim = octmps.read_deck(p["opt"], p["mci"])
+    mesh = octmps.build_mesh(p["mesh"])
+    xs = octmps.probe_positions(sim)
+    x = xs[len(xs) // 2]
+    return {"paths": p, "sim": sim, "mesh": mesh, "x": x, "root": mesh.find_root(x)}
+
+
+# A packet whose likelihood ratio turned NaN in the FP32 forms before cosines
+# were clamped: on layers_deck, seed 102, RNG lane 36485, its packet 36 (the
+# lane's 37th); its second biased scattering rotated the direction about the
+# nearly vertical probe axis, off unit length by 0.24 %, and the cosine
+# between the old and new directions came out as 1.0023.
+NAN_CASE = {"seed": 102, "lane": 36485, "packets": 37}

@@ -338,3 +338,23 @@ def test_stopped_packet_bit_exact_on_2m_tet_mesh(ctx, torch_cuda, octmps, oracle
     assert st["steps"] == t_o["steps"]
     assert_records_equal(r_g, r_o)
     assert_tallies_equal(t_g, t_o, 0, d["sim"].num_optical_depth_length_steps)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_fp32_forms_keep_the_likelihood_finite(ctx, octmps, layers_deck, precision):
+    """37 packets on each of 36,486 lanes of the four-layer slab, the last lane
+    being the one whose 37th packet had a NaN likelihood before cosines were
+    clamped: no NaN or infinite contribution, every sum finite."""
+    from conftest import NAN_CASE as S
+    d = layers_deck
+    nb = d["sim"].num_optical_depth_length_steps
+    lanes = S["lane"] + 1
+    mid = ctx.upload_mesh(d["mesh"])
+    j = ctx.submit(mid, d["sim"], d["x"], d["root"], n_photons=S["packets"] * lanes,
+                   seed=S["seed"], n_lanes=lanes, precision=precision)
+    t = ctx.fetch(j, nb)
+    ctx.release(j)
+    ctx.release_mesh(mid)
+    assert t["num_nonfinite"] == 0
+    for k in ("sum1", "sumsq1", "sum2", "sumsq2"):
+        assert np.all(np.isfinite(t[k][:nb])), k

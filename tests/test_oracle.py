@@ -171,3 +171,19 @@ def test_oracle_stops_a_packet_that_makes_no_progress(octmps, oracle, multiplier
                         1, 1, one, 0, record=True)
     assert t["capped"] == 1
     assert rec["steps"][0] == S["steps"]
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_oracle_fp32_forms_keep_the_likelihood_finite(octmps, oracle, multipliers, layers_deck,
+                                                      precision):
+    from conftest import NAN_CASE as S
+    import oracle_py
+    d = layers_deck
+    rng = octmps.rng_init(multipliers[: 3 + 3 * (S["lane"] + 1)], S["lane"] + 1, S["seed"])
+    one = {k: v[S["lane"]:S["lane"] + 1].copy() for k, v in rng.items()}
+    t = oracle.run(oracle_py.params_from_sim(d["sim"]), d["mesh"], (d["x"], 0.0, 0.0), d["root"],
+                   S["packets"], 1, one, precision)
+    nb = d["sim"].num_optical_depth_length_steps
+    assert t["num_filtered"] > 0
+    for k in ("sum1", "sumsq1", "sum2", "sumsq2"):
+        assert np.all(np.isfinite(t[k][:nb])), k
