@@ -109,8 +109,9 @@ struct Incident {
 // total number of units, so a kernel thread that takes unit u < total always
 // finds u's slot complete.  Threads take units by compare-and-swap on the
 // next-unit counter, which therefore never passes the total.  A thread that
-// finds no unit left retries for linger_us (jobs submitted meanwhile are
-// taken up by the running launch) and then exits.  Several launches may work
+// finds no unit left retries (jobs submitted meanwhile are taken up by the
+// running launch) until its block has been idle for linger_us or the host
+// raises the drain word, and then exits.  Several launches may work
 // through one table at once: the host starts another when work arrives while
 // the running one may be down to its last threads, and the new launch's
 // blocks take SM slots as the older launch's blocks leave.
@@ -118,7 +119,8 @@ struct LaunchArgs {
     const JobDesc *jobs;            // job slots
     const uint64_t *unit_base;      // [n_slots]: first unit of each slot; ~0 for empty slots
     int32_t n_slots;                // table capacity (binary search range)
-    unsigned long long *ctrl;       // [0] next unit to hand out, [1] total units, [2] error word
+    unsigned long long *ctrl;       // [0] next unit to hand out, [1] total units, [2] error
+                                    // word, [3] nonzero: idle threads exit (drain)
     uint2 *slot_state;              // per slot: x = units (RNG lanes) finished, y = launch_seq
                                     // of the launch that finished the last one; may be null
     Incident *incident;             // may be null

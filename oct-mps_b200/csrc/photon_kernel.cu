@@ -699,14 +699,18 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     // together would otherwise contend for the counter one by one).
     __shared__ unsigned long long s_first;
     __shared__ unsigned s_count;
+    // threads of this block that hold a unit (or have not yet looked for one)
+    __shared__ unsigned s_busy;
     unsigned long long first_u;
     bool first_ok;
+    if (threadIdx.x == 0) {
+        s_busy = kBlock;
+        s_first = 0;
+        s_count = 0;
+        if (args.initial_total == 0) s_count = claim_units(args.ctrl, kBlock, s_first);
+    }
+    __syncthreads();
     if (args.initial_total == 0) {
-        if (threadIdx.x == 0) {
-            s_first = 0;
-            s_count = claim_units(args.ctrl, kBlock, s_first);
-        }
-        __syncthreads();
         first_u = s_first + threadIdx.x;
         first_ok = threadIdx.x < s_count;
     } else {
@@ -716,10 +720,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     bool first_unit = true;
     // A thread that finds no unit left waits for jobs appended while the
     // launch runs: it retries after kRetryUs, doubling the interval up to
-    // kRetryMaxUs (the counter's cache line is shared by every waiting warp),
-    // and exits after linger_us without a unit (times from the global timer
-    // in 1.024 us ticks).
-    bool waiting = false;
+    // kRetryMaxUs (the counter's cache line is shared by every waiting warp).
+    // It exits once its whole block has been without work for linger_us, or
+    // at once when the host asks the launch to drain (control word 3): a
+    // block stays resident until its last thread exits, so threads leaving
+    // one by one would hold the block's SM slot for a few long lanes while
+    // new work found no free threads.  Times from the global timer in
+    // 1.024 us ticks.
+    bool waiting = false, drain = false;
     uint32_t idle_since = 0, last_try = 0, gap = kRetryUs;
 
     for (;;) {
@@ -737,19 +745,23 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
                 const uint32_t now = timer_us();
                 if (!waiting || now - last_try >= gap) {
                     got = take_unit(args.ctrl, u);
+                    if (!got) drain = __ldcv(args.ctrl + 3) != 0ull;
                     last_try = now;
                     if (waiting && gap < kRetryMaxUs) gap <<= 1;
                 }
                 if (!got) {
                     if (!waiting) {
                         waiting = true;
+                        atomicSub(&s_busy, 1u);
                         idle_since = now;
                     }
-                    if (now - idle_since >= args.linger_us) has_work = false;
+                    if (*reinterpret_cast<volatile unsigned *>(&s_busy) != 0u) idle_since = now;
+                    if (drain || now - idle_since >= args.linger_us) has_work = false;
                     else idle = true;
                 }
             }
             if (got) {
+                if (waiting) atomicAdd(&s_busy, 1u);
                 waiting = false;
                 gap = kRetryUs;
                 // the slot holding unit u: the last one whose base is <= u

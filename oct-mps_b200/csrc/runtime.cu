@@ -970,6 +970,11 @@ octmps_status octmps_ctx_synchronize(octmps_ctx *ctx) {
     for (auto &t : ctx->tables) {
         if (!t) continue;
         octmps_status st = table_step(ctx, *t);
+        if (st != OCTMPS_OK) return st;
+        if (t->running.empty()) continue;
+        // idle threads exit at once instead of lingering (drain word)
+        FILL(t->d_ctrl + 3, 1, sizeof(unsigned long long));
+        CK(cudaStreamSynchronize(ctx->stream), "drain");
         // a launch that ends with units left (jobs appended as its threads
         // were leaving) is followed by another, which this waits for too
         while (st == OCTMPS_OK && !t->running.empty()) {
@@ -977,6 +982,8 @@ octmps_status octmps_ctx_synchronize(octmps_ctx *ctx) {
             st = table_step(ctx, *t);
         }
         if (st != OCTMPS_OK) return st;
+        FILL(t->d_ctrl + 3, 0, sizeof(unsigned long long));
+        CK(cudaStreamSynchronize(ctx->stream), "drain");
     }
     return OCTMPS_OK;
 }

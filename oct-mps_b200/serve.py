@@ -29,7 +29,7 @@ class Request:
     def __init__(self, rid, kind, mesh_key, xs, photons, seed, lanes=0):
         self.rid, self.kind, self.mesh_key = rid, kind, mesh_key
         self.xs, self.photons, self.seed = xs, photons, seed
-        self.lanes = lanes    # RNG lanes per A-scan (0: the context's default)
+        self.lanes = lanes    # RNG lanes per A-scan (0: Server.lanes_for's choice)
         self.t_arrival = None
         self.t_admitted = None
         self.t_done = None
@@ -38,11 +38,20 @@ class Request:
         self.launch_ids = set()
 
 
+def lanes_for(req, max_lanes=88800):
+    """RNG lanes of each of a request's A-scans: about 8 packets per lane.
+    A lane runs its packets one after another, so a job's latency on an
+    otherwise idle GPU grows with its packets per lane; many short lanes also
+    spread one large job over every SM."""
+    return req.lanes or int(min(max_lanes, max(1, req.photons // 8)))
+
+
 class Server:
     """Admission + completion around one context (one GPU)."""
 
-    def __init__(self, ctx, meshes, poll_s=0.0005):
+    def __init__(self, ctx, meshes, poll_s=0.0005, max_lanes=88800):
         self.ctx = ctx
+        self.max_lanes = max_lanes  # the context's multiplier table covers this many lanes
         self.meshes = meshes  # key -> dict(id=mesh id, sim=Sim, mesh=Mesh, roots=dict x->root)
         self.incoming = queue.Queue()
         self.inflight = 0
@@ -63,6 +72,9 @@ class Server:
         if x not in m["roots"]:
             m["roots"][x] = m["mesh"].find_root(x)
         return m["roots"][x]
+
+    def lanes_for(self, req):
+        return lanes_for(req, self.max_lanes)
 
     def submit(self, req):
         req.t_arrival = time.perf_counter()
@@ -85,7 +97,7 @@ class Server:
                     x = pending.xs[k]
                     j = self.ctx.submit(m["id"], m["sim"], x, self.root(pending.mesh_key, x),
                                         n_photons=pending.photons, seed=pending.seed + k,
-                                        n_lanes=pending.lanes)
+                                        n_lanes=self.lanes_for(pending))
                     pending.jobs.append((j, k))
                     with self.lock:
                         self.owner[j] = (pending, k)
@@ -242,14 +254,15 @@ def main():
     args = ap.parse_args()
     work = tempfile.mkdtemp(prefix="octmps_serve_")
     meshes = build_meshes(args.scale, work)
-    mult = octmps.safeprimes(3 + 3 * 88800)
+    max_lanes = 1 << 18
+    mult = octmps.safeprimes(3 + 3 * max_lanes)
     rng = np.random.default_rng(5)
     with octmps.Context(args.device, mult) as ctx:
         for m in meshes.values():
             m["id"] = ctx.upload_mesh(m["mesh"])
         # capacity: packets/s with every request queued at once
         cal = make_stream(meshes, args.requests, 1e9, np.random.default_rng(55), args.photon_scale)
-        srv = Server(ctx, meshes)
+        srv = Server(ctx, meshes, max_lanes=max_lanes)
         wall = run_stream(srv, cal)
         cap_pkts = srv.packets_done / wall
         work_per_req = srv.packets_done / len(cal)
@@ -260,7 +273,7 @@ def main():
         for load in [float(v) for v in args.loads.split(",")]:
             rate = load * cap_pkts / work_per_req
             reqs = make_stream(meshes, args.requests, rate, rng, args.photon_scale)
-            srv = Server(ctx, meshes)
+            srv = Server(ctx, meshes, max_lanes=max_lanes)
             wall = run_stream(srv, reqs)
             srv.close()
             done = [r for _, r in reqs]

@@ -34,7 +34,7 @@ def test_served_requests_match_alone(octmps, multipliers, small_deck, small_matc
             for k, x in enumerate(r.xs):
                 root = m["mesh"].find_root(x)
                 j = ctx.submit(m["id"], m["sim"], x, root, n_photons=r.photons, seed=r.seed + k,
-                               n_lanes=r.lanes)
+                               n_lanes=serve.lanes_for(r))
                 alone[(r.rid, k)] = ctx.fetch(j, nb)
                 ctx.release(j)
         srv = serve.Server(ctx, meshes)
