@@ -190,6 +190,13 @@ def run_ours(args, rank, world, local_rank, dist):
         torch.cuda.synchronize()
 
     mid = ctx.upload_mesh(mesh)
+    tuned = None
+    if args.autotune:
+        # launch variant chosen on 4 A-scans' worth of packets at the first position
+        best, table = ctx.autotune(mid, sim, xs[0], roots[0], precision=args.precision,
+                                   n_photons=args.photons, n_jobs=4, n_lanes=lanes)
+        tuned = {"blocks_per_sm": best[0], "scatter_share": best[1],
+                 "table_steps_per_s": [[b, sh, round(v)] for b, sh, v in table]}
     for _ in range(args.warmup):
         one_step(mid)
     barrier()
@@ -302,6 +309,7 @@ def run_ours(args, rank, world, local_rank, dist):
                              f"bound by instruction issue and gather latency"},
         "clocks": clocks,
         "plain_single_job": plain,
+        "autotune": tuned,
     }
 
 
@@ -383,6 +391,8 @@ def main():
     ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--lanes", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--autotune", action="store_true",
+                    help="choose the launch variant on a sample before timing")
     ap.add_argument("--plain-ascans", type=int, default=4,
                     help="A-scans run one per launch for the batched-over-plain ratio")
     args = ap.parse_args()

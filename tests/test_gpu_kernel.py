@@ -358,3 +358,23 @@ def test_fp32_forms_keep_the_likelihood_finite(ctx, octmps, layers_deck, precisi
     assert t["num_nonfinite"] == 0
     for k in ("sum1", "sumsq1", "sum2", "sumsq2"):
         assert np.all(np.isfinite(t[k][:nb])), k
+
+
+def test_autotune_picks_a_variant_and_keeps_results(ctx, octmps, small_deck):
+    """The autotuner times each launch variant on a sample and keeps the
+    fastest; the variants change timing only, never the counts."""
+    sim = small_deck["sim"]
+    nb = sim.num_optical_depth_length_steps
+    mid = ctx.upload_mesh(small_deck["mesh"])
+    best, table = ctx.autotune(mid, sim, 0.0, small_deck["root"], n_photons=100_000,
+                               n_jobs=2, n_lanes=20_000, shares=(12, 16))
+    assert len(table) == 4 and best in table and all(r[2] > 0 for r in table)
+    runs = []
+    for b, sh in ((2, 8), (3, 24)):
+        ctx.configure(blocks_per_sm=b, scatter_share=sh)
+        j = ctx.submit(mid, sim, 0.0, small_deck["root"], n_photons=30_000, seed=3, n_lanes=3000)
+        runs.append(ctx.fetch(j, nb))
+        ctx.release(j)
+    ctx.configure(blocks_per_sm=0, scatter_share=0)
+    assert_tallies_equal(runs[0], runs[1], 0, nb)
+    ctx.release_mesh(mid)
