@@ -190,14 +190,15 @@ octmps_status octmps_ctx_set_multipliers(octmps_ctx *ctx, const uint32_t *a, uin
 /* Launch configuration (0 = autotuned / default). */
 typedef struct {
     int32_t block_size;       /* threads per block */
-    int32_t blocks_per_sm;    /* resident blocks per SM */
+    int32_t blocks_per_sm;    /* resident 256-thread blocks per SM: 2, 3 or 4 (0 = 3);
+                                 the FP64 form always runs 2 */
     int32_t default_lanes;    /* RNG lanes per job when job.n_lanes = 0 */
     int32_t use_graphs;       /* reserved, 0 (a batch is one persistent launch, so
                                  there is no launch sequence to replay) */
     uint64_t hbm_budget_bytes;/* admission budget for job state; 0 = 80% of free */
     int32_t scatter_share;    /* a warp runs its lanes' scattering step halves once at
                                  least scatter_share/32 of its live lanes wait for one
-                                 (1..32; 0 = 16) */
+                                 (1..32; 0 = 12) */
     int32_t linger_us;        /* a kernel thread that finds no work waits this long for
                                  newly submitted jobs before it exits (0 = 2000;
                                  -1 = exit at once; at most 1000000) */

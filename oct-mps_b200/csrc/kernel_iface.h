@@ -144,7 +144,7 @@ constexpr unsigned int kErrBadNeighbour = 4u; // neighbour index out of range
 enum Precision { kMixed = 0, kFP32 = 1, kFP64 = 2 };
 
 // Host-callable launcher (photon_kernel.cu).
-// min_blocks (2 or 3) selects the variant compiled for that many resident
+// min_blocks (2, 3 or 4) selects the variant compiled for that many resident
 // blocks per SM; records (test hook) selects the recording variant.
 int launch_photon_kernel(int precision, int min_blocks, const LaunchArgs &args, int grid,
                          int block, void *stream, void *records);

@@ -166,6 +166,48 @@ __device__ __forceinline__ void atomic_max_bits<float>(float *addr, float v) {
     atomicMax(reinterpret_cast<unsigned int *>(addr), __float_as_uint(v));
 }
 
+// Class I/II tally of one detection, src/octmps_kernel.cuh:684-744.  Out of
+// line (a detection is rare) and given its inputs by value: a member function
+// would take the lane's address and keep the lane's state in local memory
+// instead of registers.  Returns the number of bins the contribution went to.
+template <typename T, typename P>
+__device__ __noinline__ int tally_detection(const JobDesc *jd, P op, T max_depth, T w,
+                                            T r_fresnel, T lr) {
+    const JobDesc &J = *jd;
+    const TallyLayout L = tally_layout(J.nbins, sizeof(P));
+    unsigned char *base = reinterpret_cast<unsigned char *>(J.tally);
+    unsigned long long *totals = reinterpret_cast<unsigned long long *>(base + L.totals);
+    atomicAdd(&totals[0], 1ull);
+    const P depth = DevNum<P>::div(op, (P)2);
+    const P vpf = DevNum<P>::div(depth - (P)J.shift, (P)J.bin_width);
+    long long vp;
+    if (!(vpf > (P)0)) vp = 0;
+    else if (vpf >= (P)4294967295.0) vp = 4294967295ll;
+    else vp = (long long)vpf;
+    const bool class1 = (P)max_depth > depth - (P)J.half_lc;
+    const T c = w * ((T)1 - r_fresnel) * lr;
+    const P cp = (P)c;
+    // NaN or infinite: counted, and added like any other
+    if (!(cp - cp == (P)0)) atomicAdd(&totals[3], 1ull);
+    unsigned long long *cnt =
+        reinterpret_cast<unsigned long long *>(base + (class1 ? L.count1 : L.count2));
+    P *sum = reinterpret_cast<P *>(base + (class1 ? L.sum1 : L.sum2));
+    P *sumsq = reinterpret_cast<P *>(base + (class1 ? L.sumsq1 : L.sumsq2));
+    P *mx = reinterpret_cast<P *>(base + (class1 ? L.max1 : L.max2));
+    int n = 0;
+    for (long long ii = vp - 3; ii < vp + 3; ++ii) {
+        if (ii >= 0 && ii < J.nbins) {
+            if (ii == vp) atomicAdd(&totals[class1 ? 1 : 2], 1ull);
+            atomicAdd(&sum[ii], cp);
+            atomicAdd(&sumsq[ii], cp * cp);
+            atomic_max_bits<P>(&mx[ii], cp);
+            atomicAdd(&cnt[ii], 1ull);
+            ++n;
+        }
+    }
+    return n;
+}
+
 template <typename T, typename P, bool kRecord>
 struct Lane {
     // photon
@@ -229,43 +271,6 @@ struct Lane {
             rhash = 14695981039346656037ull;
             rsteps = rhits = rscatters = rrestores = rdetections = rsurvivals = 0;
             rcontrib = 0.0;
-        }
-    }
-
-    // Class I/II tally, src/octmps_kernel.cuh:684-744.
-    __device__ __noinline__ void tally(T r_fresnel) {
-        const JobDesc &J = *jd;
-        const TallyLayout L = tally_layout(J.nbins, sizeof(P));
-        unsigned char *base = reinterpret_cast<unsigned char *>(J.tally);
-        unsigned long long *totals = reinterpret_cast<unsigned long long *>(base + L.totals);
-        atomicAdd(&totals[0], 1ull);
-        const P depth = DevNum<P>::div(op, (P)2);
-        const P vpf = DevNum<P>::div(depth - (P)J.shift, (P)J.bin_width);
-        long long vp;
-        if (!(vpf > (P)0)) vp = 0;
-        else if (vpf >= (P)4294967295.0) vp = 4294967295ll;
-        else vp = (long long)vpf;
-        const bool class1 = (P)max_depth > depth - (P)J.half_lc;
-        const T c = w * ((T)1 - r_fresnel) * lr;
-        const P cp = (P)c;
-        // NaN or infinite: counted, and added like any other.  (Flagging the
-        // lane here instead, through a member of this out-of-line function's
-        // object, halved the kernel's speed.)
-        if (!(cp - cp == (P)0)) atomicAdd(&totals[3], 1ull);
-        unsigned long long *cnt =
-            reinterpret_cast<unsigned long long *>(base + (class1 ? L.count1 : L.count2));
-        P *sum = reinterpret_cast<P *>(base + (class1 ? L.sum1 : L.sum2));
-        P *sumsq = reinterpret_cast<P *>(base + (class1 ? L.sumsq1 : L.sumsq2));
-        P *mx = reinterpret_cast<P *>(base + (class1 ? L.max1 : L.max2));
-        for (long long ii = vp - 3; ii < vp + 3; ++ii) {
-            if (ii >= 0 && ii < J.nbins) {
-                if (ii == vp) atomicAdd(&totals[class1 ? 1 : 2], 1ull);
-                if (kRecord) rcontrib += (double)cp;
-                atomicAdd(&sum[ii], cp);
-                atomicAdd(&sumsq[ii], cp * cp);
-                atomic_max_bits<P>(&mx[ii], cp);
-                atomicAdd(&cnt[ii], 1ull);
-            }
         }
     }
 
@@ -568,7 +573,11 @@ struct Lane {
                             filt = true;
                     }
                     if (filt) {
-                        tally(r);
+                        const int nbins_added = tally_detection<T, P>(jd, op, max_depth, w, r, lr);
+                        if (kRecord) {
+                            const P cp = (P)(w * ((T)1 - r) * lr);
+                            for (int k = 0; k < nbins_added; ++k) rcontrib += (double)cp;
+                        }
                         ev |= 8;
                         if (kRecord) ++rdetections;
                     }
@@ -910,6 +919,7 @@ const void *pick(int min_blocks, bool record) {
     switch (min_blocks) {
         case 2: return (const void *)photon_kernel<T, P, false, 2>;
         case 3: return (const void *)photon_kernel<T, P, false, 3>;
+        case 4: return (const void *)photon_kernel<T, P, false, 4>;
         default: return nullptr;
     }
 }
@@ -918,7 +928,7 @@ const void *photon_kernel_fn(int precision, int min_blocks, bool record) {
     switch (precision) {
         case kMixed: return pick<float, double>(min_blocks, record);
         case kFP32: return pick<float, float>(min_blocks, record);
-        case kFP64: return pick<double, double>(min_blocks == 3 ? 2 : min_blocks, record);
+        case kFP64: return pick<double, double>(2, record);  // spills at 80 registers
         default: return nullptr;
     }
 }

@@ -58,9 +58,11 @@ namespace {
 // Resident blocks per SM the default kernel variant is compiled for, and the
 // share of a warp's live lanes (in 32nds) that must wait for the scattering
 // half of their step before the warp runs it; both the best of a sweep on
-// the B-scan workload (2 blocks: 128-register cap, no spills).
-constexpr int kDefaultMinBlocks = 2;
-constexpr int kDefaultScatterShare = 16;
+// 8 A-scans of the B-scan workload (steps/s, mixed form): 3 blocks (80-register
+// cap, 92 B spilled) 33.5 G at share 12, against 29.4 G with 2 blocks (no
+// spills) and 28.0 G with 4 (64 registers, 346 B spilled).
+constexpr int kDefaultMinBlocks = 3;
+constexpr int kDefaultScatterShare = 12;
 constexpr int kTableSlots = 4096;       // jobs per table between resets
 constexpr int kMaxLaunches = 4;         // launches in flight per table
 constexpr double kRefreshMs = 0.2;      // slot states are read back at most this often
@@ -334,9 +336,9 @@ octmps_status table_launch(octmps_ctx *ctx, Table &T) {
     if (fresh ? T.next >= T.total
               : (T.total <= T.total_at_launch || (int)T.running.size() >= kMaxLaunches))
         return OCTMPS_OK;
-    // Variant compiled for 2 or 3 resident blocks per SM (register cap
-    // 128 or 80); the FP64 form and the recording variant have only 2.
-    int min_blocks = ctx->cfg.blocks_per_sm == 2 || ctx->cfg.blocks_per_sm == 3
+    // Variant compiled for 2, 3 or 4 resident blocks per SM (register cap
+    // 128, 80 or 64); the FP64 form and the recording variant have only 2.
+    int min_blocks = ctx->cfg.blocks_per_sm >= 2 && ctx->cfg.blocks_per_sm <= 4
                          ? ctx->cfg.blocks_per_sm
                          : kDefaultMinBlocks;
     if (T.prec == kFP64 || ctx->record_buf) min_blocks = 2;
