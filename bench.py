@@ -40,6 +40,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "oct-mps_b200"))
 
 B_STEP = 80  # algorithmic bytes per propagation step: 4 float4 planes + int4 neighbours
+# DRAM traffic of one launch, from an ncu capture (dram__bytes_read.sum + write) of 8 A-scans
+# x 2e5 packets on the B-scan mesh: 65.1 MB = the mesh once (30.5 MB) + 4.33 MB per A-scan
+# (its 88,800 RNG lanes, 3.2 MB, its tally and job state, write-backs).  The traffic does not
+# grow with packets or steps (the mesh stays in L2), so a launch's is modelled as
+# mesh + A-scans x per-A-scan bytes.
+DRAM_PER_ASCAN = (65.1e6 - 30.5e6) / 8
 
 
 def env_int(k, d):
@@ -302,7 +308,12 @@ def run_ours(args, rank, world, local_rank, dist):
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms_step},
         "gpu_launches": args.steps * 1,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak,
+                     "traffic": mesh.n_tets * 80 + batch * DRAM_PER_ASCAN,
+                     "traffic_note": "DRAM bytes per launch, modelled from an ncu capture of "
+                                     "8 A-scans x 2e5 packets (mesh once + per-A-scan state); "
+                                     "far below the algorithmic bytes because the mesh is "
+                                     "L2-resident",
                      "note": f"algorithmic {B_STEP} B per propagation step x steps per launch / "
                              f"launch time; peak = {peak_kind} HBM copy bandwidth; the mesh "
                              f"({mesh.n_tets * 80 / 1e6:.0f} MB) is L2-resident, the kernel is "
