@@ -685,7 +685,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     // packets per lane below 2^32) and steps of the current packet (capped
     // at step_cap <= 2^32)
     uint32_t packets_left = 0, steps_packet = 0;
-    uint64_t record_lane = ~0ull;  // lane whose first packet is being recorded
+    uint32_t record_lane = ~0u;  // lane of the current unit (lane counts are 32-bit)
     bool recording = false;
 
     // Lanes of this warp still in the loop, and whether this lane's current
@@ -812,7 +812,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
                     steps_packet = 0;
                     pending = false;
                     recording = kRecord && records && lo == args.record_slot;
-                    record_lane = v;
+                    record_lane = (uint32_t)v;
                 }
             }
         }
