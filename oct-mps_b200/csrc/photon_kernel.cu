@@ -685,7 +685,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     // packets per lane below 2^32) and steps of the current packet (capped
     // at step_cap <= 2^32)
     uint32_t packets_left = 0, steps_packet = 0;
-    uint32_t record_lane = ~0u;  // lane of the current unit (lane counts are 32-bit)
     bool recording = false;
 
     // Lanes of this warp still in the loop, and whether this lane's current
@@ -701,7 +700,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     bool pending = false;
     const int share = args.scatter_share;
     unsigned int *const err = reinterpret_cast<unsigned int *>(args.ctrl + 2);
-    int slot = 0;  // job slot of the current unit
     // First units: in a launch started on an idle table, thread t takes unit
     // start_unit + t; in one started beside a running launch, each block
     // claims a run of units at once (a grid's worth of threads arriving
@@ -736,8 +734,22 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     // one by one would hold the block's SM slot for a few long lanes while
     // new work found no free threads.  Times from the global timer in
     // 1.024 us ticks.
-    bool waiting = false, drain = false;
-    uint32_t idle_since = 0, last_try = 0, gap = kRetryUs;
+    // This state, and the current unit's job slot and lane, are touched only
+    // between units (and at a stop), so they live in shared memory rather
+    // than in registers the propagation loop needs.
+    struct UnitState {
+        uint32_t idle_since, last_try, gap;
+        int32_t slot;   // job slot of the current unit
+        uint32_t lane;  // its RNG lane (lane counts are 32-bit)
+        bool waiting, drain;
+    };
+    __shared__ UnitState s_unit[kBlock];
+    UnitState &lg = s_unit[threadIdx.x];
+    lg.waiting = lg.drain = false;
+    lg.idle_since = lg.last_try = 0;
+    lg.gap = kRetryUs;
+    lg.slot = 0;
+    lg.lane = ~0u;
 
     for (;;) {
         bool has_work = true;
@@ -752,27 +764,27 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
             }
             if (!got) {
                 const uint32_t now = timer_us();
-                if (!waiting || now - last_try >= gap) {
+                if (!lg.waiting || now - lg.last_try >= lg.gap) {
                     got = take_unit(args.ctrl, u);
-                    if (!got) drain = __ldcv(args.ctrl + 3) != 0ull;
-                    last_try = now;
-                    if (waiting && gap < kRetryMaxUs) gap <<= 1;
+                    if (!got) lg.drain = __ldcv(args.ctrl + 3) != 0ull;
+                    lg.last_try = now;
+                    if (lg.waiting && lg.gap < kRetryMaxUs) lg.gap <<= 1;
                 }
                 if (!got) {
-                    if (!waiting) {
-                        waiting = true;
+                    if (!lg.waiting) {
+                        lg.waiting = true;
                         atomicSub(&s_busy, 1u);
-                        idle_since = now;
+                        lg.idle_since = now;
                     }
-                    if (*reinterpret_cast<volatile unsigned *>(&s_busy) != 0u) idle_since = now;
-                    if (drain || now - idle_since >= args.linger_us) has_work = false;
+                    if (*reinterpret_cast<volatile unsigned *>(&s_busy) != 0u) lg.idle_since = now;
+                    if (lg.drain || now - lg.idle_since >= args.linger_us) has_work = false;
                     else idle = true;
                 }
             }
             if (got) {
-                if (waiting) atomicAdd(&s_busy, 1u);
-                waiting = false;
-                gap = kRetryUs;
+                if (lg.waiting) atomicAdd(&s_busy, 1u);
+                lg.waiting = false;
+                lg.gap = kRetryUs;
                 // the slot holding unit u: the last one whose base is <= u
                 // (bases of empty slots are ~0); read past L1, the host may
                 // have filled the slot after this launch started
@@ -782,7 +794,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
                     if (__ldcg(args.unit_base + mid) <= u) lo = mid;
                     else hi = mid - 1;
                 }
-                slot = lo;
+                lg.slot = lo;
                 const JobDesc *jd = args.jobs + lo;
                 const uint64_t v = u - __ldcg(args.unit_base + lo);
                 if (jd != L.jd) {
@@ -806,13 +818,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
                 packets_left = (uint32_t)(jd->n_photons / nl + (v < jd->n_photons % nl ? 1 : 0));
                 if (packets_left == 0) {
                     idle = true;  // a lane without packets: take another unit next time
-                    unit_finished(args, slot, jd->n_lanes);
+                    unit_finished(args, lg.slot, jd->n_lanes);
                 } else {
                     L.launch();
                     steps_packet = 0;
                     pending = false;
                     recording = kRecord && records && lo == args.record_slot;
-                    record_lane = (uint32_t)v;
+                    lg.lane = (uint32_t)v;
                 }
             }
         }
@@ -860,10 +872,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
         if (reason) {
             Incident *inc = args.incident;
             if (inc && atomicCAS(&inc->flag, 0u, reason) == 0u) {
-                inc->slot = (unsigned)slot;
+                inc->slot = (unsigned)lg.slot;
                 inc->tet = L.tet;
                 inc->packets_left = packets_left;
-                inc->lane = record_lane;
+                inc->lane = lg.lane;
                 inc->steps = steps_packet;
                 inc->pos[0] = (double)L.x;
                 inc->pos[1] = (double)L.y;
@@ -895,7 +907,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
                 r.survivals = L.rsurvivals;
                 r.contribution = L.rcontrib;
                 r.optical_path = (double)L.op;
-                records[record_lane] = r;
+                records[lg.lane] = r;
                 recording = false;
             }
             --packets_left;
@@ -903,7 +915,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
                 L.launch();
                 steps_packet = 0;
             } else {
-                unit_finished(args, slot, L.jd->n_lanes);
+                unit_finished(args, lg.slot, L.jd->n_lanes);
             }
         }
     }
