@@ -59,8 +59,8 @@ namespace {
 // share of a warp's live lanes (in 32nds) that must wait for the scattering
 // half of their step before the warp runs it; both the best of a sweep on
 // 8 A-scans of the B-scan workload (steps/s, mixed form): 3 blocks (80-register
-// cap, 92 B spilled) 33.5 G at share 12, against 29.4 G with 2 blocks (no
-// spills) and 28.0 G with 4 (64 registers, 346 B spilled).
+// cap, 44 B spilled) 33.0-33.6 G at shares 10-14, against 28.8-29.3 G with 2
+// blocks (no spills) and 28.4-29.1 G with 4 (64 registers, 228 B spilled).
 constexpr int kDefaultMinBlocks = 3;
 constexpr int kDefaultScatterShare = 12;
 constexpr int kTableSlots = 4096;       // jobs per table between resets
