@@ -13,8 +13,9 @@
 // the launch runs is appended to the table and taken up by the running
 // kernel as its threads free up (continuous batching), so its work overlaps
 // the work already on the GPU.  A kernel thread that finds no unit left
-// waits (linger_us, retrying) for new jobs before it exits, so a stream of
-// submissions keeps one launch at full width.  A launch whose threads have
+// keeps retrying for new jobs while any thread of its block has work and
+// then for linger_us, and exits early only when the host drains the launch,
+// so a stream of submissions keeps one launch at full width.  A launch whose threads have
 // begun to leave may be down to a few of them; work arriving then also
 // starts another launch over the same table (up to kMaxLaunches at once,
 // each on its own stream), whose blocks take SM slots as the older launch's
