@@ -286,13 +286,19 @@ octmps_status octmps_write_result(const char *dir, const octmps_sim *sim, double
  * process exits.  The first call on a device looks up that array's device
  * address (once per device); make that first call before any stream capture.
  * All calls on a device share the array, so calls whose work overlaps on the
- * GPU race: serialise them.  The call returns after the A-scan finished.
+ * GPU race: serialise them.  The array's device address is kept per device
+ * for the life of the process, so calls after cudaDeviceReset are not
+ * supported.  The call returns after the A-scan finished.
  *
  * Device layouts the caller provides:
  *   planes : float, 16 per tet: for face k = 0..3 the reference's face plane
  *            (Nx, Ny, Nz, d) of tet_faces[k] times tet_signs[k]
  *   adj    : int32, 4 per tet (16-byte aligned): -1 for a boundary face, else
- *            neighbour | region_of_neighbour << 24 (meshes below 2^24 tets)
+ *            neighbour | region_of_neighbour << 24 (meshes below 2^24 tets),
+ *            with neighbour < n_tets and 1 <= region < sim->n_regions; the
+ *            call does not read this array on the host: the kernel checks
+ *            each entry it follows and, on a bad one, ends that packet and
+ *            the call returns OCTMPS_ERR_KERNEL
  *   rng_*  : the lanes' generator states as octmps_rng_init fills them
  *   tally  : OCTMPS_NOALLOC_TALLY_BYTES(nbins) bytes, zeroed by the call:
  *            uint64 totals[4] (filtered, class I, class II, 0) at byte 0, then
@@ -315,7 +321,10 @@ typedef struct {
     const int32_t *adj;             /* device */
     int32_t n_tets;
     int32_t root_tet;               /* octmps_mesh_find_root */
-    int32_t root_region;            /* region of root_tet */
+    int32_t root_region;            /* region of root_tet (tet_region[root_tet] of the
+                                       mesh; it sets the specular weight and the
+                                       first optical constants, and is not checked
+                                       against adj) */
     double probe_x, probe_y, probe_z;
     uint64_t n_photons;
     uint32_t n_lanes;               /* 1 .. n_photons */

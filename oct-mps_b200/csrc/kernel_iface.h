@@ -51,6 +51,7 @@ struct alignas(256) JobDesc {
     double n_ambient;
     double shift, bin_width, half_lc;  // OpticalDepthShift, Lc/6, Lc/2 (round-down)
     int32_t root_tet, root_region, type_bias, nbins;
+    int32_t n_regions;    // entries of regions[]; a neighbour's region must be below it
 };
 
 static_assert(sizeof(JobDesc) == 256, "a job slot is two cache lines");
@@ -142,6 +143,14 @@ constexpr unsigned int kErrStepCap = 2u;      // a packet exceeded step_cap
 constexpr unsigned int kErrBadNeighbour = 4u; // neighbour index out of range
 
 enum Precision { kMixed = 0, kFP32 = 1, kFP64 = 2 };
+
+// Resident blocks per SM of the default kernel variant, and the share of a
+// warp's live lanes (in 32nds) that must wait for the scattering half of
+// their step before the warp runs it: the best of a sweep on 8 A-scans of the
+// B-scan workload (steps/s, mixed form): 3 blocks (80-register cap) 33.0-33.6 G
+// at shares 10-14, against 28.8-29.3 G with 2 blocks and 28.4-29.1 G with 4.
+constexpr int kDefaultMinBlocks = 3;
+constexpr int kDefaultScatterShare = 12;
 
 // Host-callable launcher (photon_kernel.cu).
 // min_blocks (2, 3 or 4) selects the variant compiled for that many resident

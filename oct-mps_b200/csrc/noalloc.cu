@@ -48,7 +48,10 @@ std::mutex g_mu;
 unsigned char *g_scratch_addr[kMaxDevices] = {nullptr};
 
 // Device address of the scratch array on the current device (looked up once
-// per device; the host-side symbol is not a device address).
+// per device; the host-side symbol is not a device address).  The address is
+// kept for the life of the process: after cudaDeviceReset (or anything else
+// that replaces the device's primary context) it is stale, and calls on that
+// device are not supported.
 cudaError_t scratch_address(int device, unsigned char **out) {
     std::lock_guard<std::mutex> g(g_mu);
     if (!g_scratch_addr[device]) {
@@ -144,6 +147,7 @@ extern "C" octmps_status octmps_ascan_run_noalloc(const octmps_noalloc_ascan *a,
     D.half_lc = div_rd_host(s.coherence_length_source, 2.0);
     D.root_tet = a->root_tet;
     D.root_region = a->root_region;
+    D.n_regions = s.n_regions;
     D.type_bias = s.type_bias;
     D.nbins = s.num_optical_depth_length_steps;
     memcpy(img + kJobOff, &D, sizeof D);
@@ -154,7 +158,8 @@ extern "C" octmps_status octmps_ascan_run_noalloc(const octmps_noalloc_ascan *a,
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
         return OCTMPS_ERR_DEVICE;
     int regs = 0, per_sm = 0;
-    if (photon_kernel_attributes(kMixed, 256, 2, &regs, &per_sm) != 0 || per_sm < 1) per_sm = 1;
+    if (photon_kernel_attributes(kMixed, 256, kDefaultMinBlocks, &regs, &per_sm) != 0 || per_sm < 1)
+        per_sm = 1;
     uint64_t grid = (uint64_t)sms * per_sm;
     const uint64_t useful = (a->n_lanes + 255) / 256;
     if (grid > useful) grid = useful;
@@ -180,11 +185,11 @@ extern "C" octmps_status octmps_ascan_run_noalloc(const octmps_noalloc_ascan *a,
     L.start_unit = 0;
     L.initial_total = a->n_lanes;
     L.step_cap = 1ull << 26;
-    L.scatter_share = 10;
+    L.scatter_share = kDefaultScatterShare;
     L.launch_seq = 1;
     L.record_slot = -1;
     L.linger_us = 0;
-    if (launch_photon_kernel(kMixed, 2, L, (int)grid, 256, st, nullptr) != 0)
+    if (launch_photon_kernel(kMixed, kDefaultMinBlocks, L, (int)grid, 256, st, nullptr) != 0)
         return OCTMPS_ERR_DEVICE;
     unsigned int err = 0;
     if (cudaMemcpyAsync(&err, scratch + kCtrlOff + 16, sizeof err, cudaMemcpyDeviceToHost, st) != cudaSuccess ||

@@ -521,6 +521,14 @@ struct Lane {
             const T ca1 = -min_cos;
             const int32_t entry = face == 0 ? nb.x : face == 1 ? nb.y : face == 2 ? nb.z : nb.w;
             const int next_region = entry < 0 ? 0 : (int)((uint32_t)entry >> kAdjIndexBits);
+            // A neighbour entry must name a tet of the mesh and a region of
+            // the job's table: the job API checks the mesh at upload, the
+            // allocation-free entry point takes the caller's array unchecked.
+            if (entry >= 0 && (next_region >= jd->n_regions ||
+                               (int32_t)((uint32_t)entry & kAdjIndexMask) >= jd->n_tets)) {
+                atomicOr(err, kErrBadNeighbour);
+                return kEnd;
+            }
             const T nt = entry < 0 ? (T)jd->n_ambient
                                    : __ldg(reinterpret_cast<const T *>(regions + next_region));
             T r;

@@ -56,14 +56,6 @@ using namespace octmps;
 
 namespace {
 
-// Resident blocks per SM the default kernel variant is compiled for, and the
-// share of a warp's live lanes (in 32nds) that must wait for the scattering
-// half of their step before the warp runs it; both the best of a sweep on
-// 8 A-scans of the B-scan workload (steps/s, mixed form): 3 blocks (80-register
-// cap, 44 B spilled) 33.0-33.6 G at shares 10-14, against 28.8-29.3 G with 2
-// blocks (no spills) and 28.4-29.1 G with 4 (64 registers, 228 B spilled).
-constexpr int kDefaultMinBlocks = 3;
-constexpr int kDefaultScatterShare = 12;
 constexpr int kTableSlots = 4096;       // jobs per table between resets
 constexpr int kMaxLaunches = 4;         // launches in flight per table
 constexpr double kRefreshMs = 0.2;      // slot states are read back at most this often
@@ -938,6 +930,7 @@ octmps_status octmps_job_submit(octmps_ctx *ctx, const octmps_job *job, octmps_j
     D.half_lc = div_rd(s.coherence_length_source, 2.0);
     D.root_tet = job->root_tet;
     D.root_region = m.region[job->root_tet];
+    D.n_regions = s.n_regions;
     D.type_bias = s.type_bias;
     D.nbins = s.num_optical_depth_length_steps;
 

@@ -230,6 +230,9 @@ class Reference:
         L.ref_mesh_counts.argtypes = [C.c_char_p, P(C.c_int32), P(C.c_int32)]
         L.ref_mesh_build.argtypes = [C.c_char_p, C.c_double, C.c_double, C.c_double,
                                      P(C.c_int32), P(C.c_double), P(C.c_int32)]
+        L.ref_mesh_build_roots.restype = C.c_int
+        L.ref_mesh_build_roots.argtypes = [C.c_char_p, C.c_int32, P(C.c_double), P(C.c_int32),
+                                           P(C.c_double), P(C.c_int32)]
         L.ref_run.restype = C.c_int
         L.ref_run.argtypes = [P(RefSim), P(RefMesh), C.c_double, C.c_double, C.c_double,
                               C.c_uint32, P(C.c_uint64), P(C.c_uint32), P(C.c_uint64),
@@ -277,6 +280,28 @@ class Reference:
         return {"idx": tet[:, 0].copy(), "region": tet[:, 1].copy(),
                 "faces": tet[:, 2:6].copy(), "signs": tet[:, 6:10].copy(),
                 "adj": tet[:, 10:14].copy(), "planes": face.reshape(-1, 4), "root": root.value,
+                "n_vertices": nv.value}
+
+    def build_mesh_roots(self, mesh_path, probe_xs):
+        """MeshGraph + SerializeGraph once and the root tet of each probe position
+        (x, 0, 0), with the reference's own functions (O(T^2) in the tet count:
+        about an hour at 381k tets).  Returns the serialised arrays, the faces
+        trimmed to the distinct ones, and the roots (-1 where none is found)."""
+        nv, nt = C.c_int32(), C.c_int32()
+        self.L.ref_mesh_counts(os.fsencode(mesh_path), C.byref(nv), C.byref(nt))
+        T = nt.value
+        tet = np.zeros(T * 14, np.int32)
+        face = np.zeros(4 * T * 4, np.float64)
+        xs = np.ascontiguousarray(probe_xs, np.float64)
+        roots = np.full(len(xs), -1, np.int32)
+        st = self.L.ref_mesh_build_roots(os.fsencode(mesh_path), len(xs), _ptr(xs, C.c_double),
+                                         _ptr(tet, C.c_int32), _ptr(face, C.c_double),
+                                         _ptr(roots, C.c_int32))
+        if st != 0:
+            raise RuntimeError(f"reference mesh build failed: {st}")
+        tet = tet.reshape(T, 14)
+        n_faces = int(tet[:, 2:6].max()) + 1
+        return {"tet": tet, "planes": face.reshape(-1, 4)[:n_faces].copy(), "roots": roots,
                 "n_vertices": nv.value}
 
     @staticmethod

@@ -217,6 +217,56 @@ int ref_mesh_build(const char *mesh_path, double probe_x, double probe_y, double
     return 0;
 }
 
+// MeshGraph + SerializeGraph once, then FindRootofGraph for each of n_probes
+// probe positions (x, 0, 0), as main() chains them for a B-scan
+// (src/main.cu:943-963, 948-955).  FindRootofGraph loops over
+// SimulationStruct::num_tetrahedrons, a short (src/octmps.h:95), which
+// wraps for meshes above 32,767 tets; the search here runs the same
+// function over the first min(T, 32767) tets, which is the reference's
+// result with a wide counter whenever the root lies among them (the
+// generated meshes write the probe's surface layer first).  roots[k] = -1
+// where it returns no tet.  tet_out: [n_tets*14]; face_out: [4*n_tets*4].
+int ref_mesh_build_roots(const char *mesh_path, int32_t n_probes, const double *probe_x,
+                         int32_t *tet_out, double *face_out, int32_t *roots) {
+    int nv = 0, nt = 0;
+    if (!read_mesh_param((char *)mesh_path, &nv, &nt)) return 1;
+    SimulationStruct sim;
+    memset(&sim, 0, sizeof sim);
+    SimulationStruct *psim = &sim;
+    TetrahedronStruct *graph = MeshGraph((char *)mesh_path, &psim);
+    if (!graph) return 2;
+    sim.num_tetrahedrons = (short)(nt < 32767 ? nt : 32767);
+    for (int32_t k = 0; k < n_probes; ++k) {
+        sim.probe_x = probe_x[k];
+        sim.probe_y = 0.0;
+        sim.probe_z = 0.0;
+        TetrahedronStruct *r = FindRootofGraph(graph, &psim);
+        roots[k] = r ? r->index : -1;
+    }
+    std::vector<Vertex> verts(nv);
+    std::vector<TriangleFaces> faces(4 * (size_t)nt);
+    memset(faces.data(), 0, faces.size() * sizeof(TriangleFaces));
+    std::vector<TetrahedronStructGPU> tets(nt);
+    SerializeGraph(graph, nv, 4 * nt, nt, verts.data(), faces.data(), tets.data());
+    for (int i = 0; i < nt; ++i) {
+        int32_t *t = tet_out + 14 * (size_t)i;
+        t[0] = tets[i].idx;
+        t[1] = tets[i].region;
+        for (int k = 0; k < 4; ++k) {
+            t[2 + k] = tets[i].faces[k];
+            t[6 + k] = tets[i].signs[k];
+            t[10 + k] = tets[i].adjTetras[k];
+        }
+    }
+    for (size_t i = 0; i < faces.size(); ++i) {
+        face_out[4 * i + 0] = faces[i].Nx;
+        face_out[4 * i + 1] = faces[i].Ny;
+        face_out[4 * i + 2] = faces[i].Nz;
+        face_out[4 * i + 3] = faces[i].d;
+    }
+    return 0;
+}
+
 // One A-scan through the reference's kernels, as RunGPUi does it
 // (src/main.cu:43-660): InitDeviceConstantMemory, InitThreadState over the
 // grid, then OCTMPSKernel relaunched until n_photons_left reaches 0

@@ -6,7 +6,20 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REF_INPUT = "/root/reference/input"
+
+
+def _reference_tree():
+    """Root of the reference's tree: OCTMPS_REFERENCE, else the tree the host
+    build in oracle/_ref/ was compiled from (absent on machines without it)."""
+    tree = os.environ.get("OCTMPS_REFERENCE", "")
+    if not tree:
+        rec = os.path.join(ROOT, "oracle", "_ref", "REF_TREE")
+        if os.path.exists(rec):
+            tree = open(rec).read().strip()
+    return tree
+
+
+REF_INPUT = os.path.join(_reference_tree(), "input") if _reference_tree() else ""
 sys.path.insert(0, os.path.join(ROOT, "oct-mps_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
@@ -76,7 +89,7 @@ def ref_deck_paths(name):
     decks = json.load(open(os.path.join(GOLDEN, "decks.json")))
     files = decks[name]["files"]
     paths = [os.path.join(REF_INPUT, f) for f in files]
-    if not all(os.path.exists(p) for p in paths):
+    if not REF_INPUT or not all(os.path.exists(p) for p in paths):
         pytest.skip("reference input decks not present")
     return paths
 

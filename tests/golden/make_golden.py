@@ -7,7 +7,9 @@ in place): its init_RNG, read_simulation_data + Bias_Read, MeshGraph +
 FindRootofGraph + SerializeGraph, the per-photon routine of OCTMPSKernel
 and its output writers.  Run it where the reference tree exists:
 
-    python tests/golden/make_golden.py [--ref-input /root/reference/input]
+    OCTMPS_REFERENCE=<reference tree> python tests/golden/make_golden.py [--ref-input DIR]
+
+(--ref-input defaults to the input/ directory of that tree.)
 
 The multiplier table comes from the project's generator (the reference's
 safeprimes_base32.txt is not shipped); fixtures record which entries they
@@ -67,7 +69,9 @@ def sim_dict(rs):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-input", default="/root/reference/input")
+    tree = os.environ.get("OCTMPS_REFERENCE", "")
+    ap.add_argument("--ref-input", default=os.path.join(tree, "input") if tree else None,
+                    required=not tree)
     args = ap.parse_args()
     R = oracle_py.Reference()
     work = tempfile.mkdtemp()

@@ -47,25 +47,15 @@ def parse_tally(raw, nb):
     return out
 
 
-def test_noalloc_entry_point_matches_job_api(octmps, small_deck):
-    torch = pytest.importorskip("torch")
-    assert torch.cuda.is_available()
-    sim, mesh, root = small_deck["sim"], small_deck["mesh"], small_deck["root"]
+def noalloc_call(octmps, torch, sim, mesh, root, lanes, n, seed, mult, adj_override=None):
+    """Caller-owned device buffers in the documented layouts, the argument
+    block and the bound entry point.  Returns (args, buffers, function, stream)."""
     nb = sim.num_optical_depth_length_steps
-    lanes, n, seed = 2000, 20000, 5
-    mult = octmps.safeprimes(3 + 3 * lanes)
-
-    # the existing entry point
-    with octmps.Context(0, mult) as ctx:
-        mid = ctx.upload_mesh(mesh)
-        jid = ctx.submit(mid, sim, sim.start_x, root, n_photons=n, seed=seed, n_lanes=lanes)
-        want = ctx.fetch(jid, nb)
-        ctx.release(jid)
-
-    # caller-owned device buffers in the documented layouts
     planes = (mesh.planes[mesh.faces] * mesh.signs[:, :, None]).astype(np.float32)
     adj = mesh.adj.astype(np.int64)
     adj = np.where(adj < 0, -1, adj | (mesh.region[np.maximum(adj, 0)].astype(np.int64) << 24))
+    if adj_override is not None:
+        adj = adj_override(adj)
     adj = adj.astype(np.uint32).view(np.int32)
     rng = octmps.rng_init(mult, lanes, seed)
     dev = {
@@ -91,11 +81,28 @@ def test_noalloc_entry_point_matches_job_api(octmps, small_deck):
     a.rng_xS, a.rng_aS = dev["xS"].data_ptr(), dev["aS"].data_ptr()
     a.tally = dev["tally"].data_ptr()
 
-    L = octmps.lib()
-    f = L.octmps_ascan_run_noalloc
+    f = octmps.lib().octmps_ascan_run_noalloc
     f.restype = C.c_int
     f.argtypes = [C.POINTER(NoallocAscan), C.c_void_p]
-    stream = torch.cuda.current_stream().cuda_stream
+    return a, dev, f, torch.cuda.current_stream().cuda_stream
+
+
+def test_noalloc_entry_point_matches_job_api(octmps, small_deck):
+    torch = pytest.importorskip("torch")
+    assert torch.cuda.is_available()
+    sim, mesh, root = small_deck["sim"], small_deck["mesh"], small_deck["root"]
+    nb = sim.num_optical_depth_length_steps
+    lanes, n, seed = 2000, 20000, 5
+    mult = octmps.safeprimes(3 + 3 * lanes)
+
+    # the existing entry point
+    with octmps.Context(0, mult) as ctx:
+        mid = ctx.upload_mesh(mesh)
+        jid = ctx.submit(mid, sim, sim.start_x, root, n_photons=n, seed=seed, n_lanes=lanes)
+        want = ctx.fetch(jid, nb)
+        ctx.release(jid)
+
+    a, dev, f, stream = noalloc_call(octmps, torch, sim, mesh, root, lanes, n, seed, mult)
     for call in range(2):  # the scratch keeps the previous call's contents
         st = f(C.byref(a), C.c_void_p(stream))
         assert st == 0, (st, octmps.STATUS.get(st))
@@ -116,3 +123,27 @@ def test_noalloc_entry_point_matches_job_api(octmps, small_deck):
     big.n_regions = 101
     a.sim = C.cast(C.pointer(big), C.c_void_p)
     assert f(C.byref(a), C.c_void_p(stream)) == 1
+
+
+def test_noalloc_bad_neighbour_entries_are_reported(octmps, small_deck):
+    """The caller's neighbour array is not read on the host; the kernel checks
+    each entry it follows.  Both cases keep every access in bounds even
+    without the check (a region below the fixed table's 100 entries; arrays
+    allocated for the whole mesh while n_tets claims half of it), so the test
+    shows the report, not a fault."""
+    torch = pytest.importorskip("torch")
+    assert torch.cuda.is_available()
+    sim, mesh, root = small_deck["sim"], small_deck["mesh"], small_deck["root"]
+    lanes, n, seed = 500, 1000, 9
+    mult = octmps.safeprimes(3 + 3 * lanes)
+    bad_region = sim.n_regions  # one past the job's regions
+    a, dev, f, stream = noalloc_call(
+        octmps, torch, sim, mesh, root, lanes, n, seed, mult,
+        adj_override=lambda adj: np.where(adj < 0, -1, (adj & 0xFFFFFF) | (bad_region << 24)))
+    assert f(C.byref(a), C.c_void_p(stream)) == 9  # OCTMPS_ERR_KERNEL
+    a, dev, f, stream = noalloc_call(octmps, torch, sim, mesh, root, lanes, n, seed, mult)
+    assert root < mesh.n_tets // 2
+    a.n_tets = mesh.n_tets // 2  # neighbours in the second half are out of range
+    assert f(C.byref(a), C.c_void_p(stream)) == 9
+    a.n_tets = mesh.n_tets  # the next call starts clean
+    assert f(C.byref(a), C.c_void_p(stream)) == 0
