@@ -21,10 +21,16 @@ launch, and the download of every A-scan's tallies, wall-clock per step.
 Under torchrun each rank runs its own B-scan (seeds offset by rank): weak
 scaling, no collective on the data path.
 
+roofline: issue-bound; algorithmic FLOPs per propagation step (frozen from
+the oracle's operation census on this workload) x steps/s against the
+non-tensor FP32 peak at the sampled clock.
+
 --impl reference times the reference's own per-photon routine
-(src/octmps_kernel.cuh, compiled for the host with OpenMP in
-oracle/_ref/) on all host cores, on a bounded sample of the same workload
-(one A-scan of the same mesh and parameters).
+(src/octmps_kernel.cuh relaunched as src/main.cu:572-623 does, compiled for
+the host with OpenMP in oracle/_ref/) on all host cores: step k runs the
+A-scans of the GPU arm's k-th launch with --ref-packets packets each, on the
+mesh the reference's own MeshGraph builds (oracle/ref_mesh_cache.py), without
+loading the product library.
 """
 import argparse
 import json
@@ -39,7 +45,16 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "oct-mps_b200"))
 
+METRIC = "photon packets/s (B-scan, 256 A-scans)"
 B_STEP = 80  # algorithmic bytes per propagation step: 4 float4 planes + int4 neighbours
+# Algorithmic FLOPs per propagation step on this workload, frozen from the
+# oracle's operation census (oracle/census.cpp: + - x / sqrt count 1, a fused
+# multiply-add 2, a transcendental 1; 1000 lanes x 2 packets at positions 0,
+# 64, 128, 192 and 255 of the B-scan, 1.39e8 steps): mixed form 65.85 FP32 +
+# 1.00 FP64, FP64 form 81.63.  tests/test_oracle.py re-counts a sample.
+F_STEP = {0: 66.85, 1: 66.85, 2: 81.63}
+F_STEP_FP64 = F_STEP[2]
+N_SM = 148
 # DRAM traffic of one launch, from an ncu capture (dram__bytes_read.sum + write) of 8 A-scans
 # x 2e5 packets on the B-scan mesh: 65.1 MB = the mesh once (30.5 MB) + 4.33 MB per A-scan
 # (its 88,800 RNG lanes, 3.2 MB, its tally and job state, write-backs).  The traffic does not
@@ -55,12 +70,19 @@ def env_int(k, d):
         return d
 
 
-def measured_peaks():
+def measured_hbm():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         d = json.load(open(p))
         return d.get("hbm_gbs", 6650.0), "measured"
     return 6650.0, "fallback"
+
+
+def fp_peak_tflops(clocks, bits):
+    """Non-tensor FMA peak at the sampled SM clock: 148 SMs x 128 FP32 (or 64
+    FP64) lanes x 2 FLOPs per cycle."""
+    mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    return N_SM * (128 if bits == 32 else 64) * 2 * mhz * 1e6 / 1e12
 
 
 class ClockSampler:
@@ -148,8 +170,20 @@ def rel_error_at_peak(t, n):
             float(np.mean(se[ok] / m[ok])) if ok.any() else None)
 
 
+def workload_config(args, n_xs, batch, n_tets=380928):
+    return {
+        "workload": f"bscan ellipsoid+2 spheres, {n_tets} tets, {n_xs} A-scans x "
+                    f"{args.photons} packets, seeds 1..{n_xs}; one step = {batch} A-scans "
+                    f"in one launch",
+        "ascans_per_step": batch,
+        "precision": {0: "mixed FP32 geometry / FP64 path+tally", 1: "FP32",
+                      2: "FP64"}[args.precision],
+        "parallelism": "weak (A-scan batches per rank)",
+        "l2": "256 MB buffer written between timed steps",
+    }
+
+
 def run_ours(args, rank, world, local_rank, dist):
-    import numpy as np
     import octmps
     import torch
 
@@ -161,22 +195,21 @@ def run_ours(args, rank, world, local_rank, dist):
     mult = octmps.safeprimes(3 + 3 * lanes)
     ctx = octmps.Context(local_rank, mult)
     flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
-
     batch = min(args.batch, len(xs))
     counter = [0]
 
-    def one_step(resident_mid):
-        """Submits the next batch of A-scans of the B-scan (positions k*batch ..
-        k*batch+batch-1, wrapping at the end of the scan), runs them in one
-        persistent launch and fetches every tally.  Returns device ms of the
-        launch, wall ms, packets, steps and the tallies."""
-        first = (counter[0] * batch) % len(xs)
-        counter[0] += 1
-        sel = [(first + k) % len(xs) for k in range(batch)]
+    def run_batch(mid, sel, precision):
+        """Submits the A-scans `sel`, runs them in one persistent launch and
+        fetches every tally.  Returns device ms of the launch, wall ms,
+        packets, propagation steps, tallies and stats.  Fails loudly if the
+        batch did not run in exactly one launch (the device time is that
+        launch's)."""
         t0 = time.perf_counter()
-        mid = resident_mid if resident_mid is not None else ctx.upload_mesh(mesh)
+        own = mid is None
+        if own:
+            mid = ctx.upload_mesh(mesh)
         ids = [ctx.submit(mid, sim, xs[k], roots[k], n_photons=args.photons,
-                          seed=rank * len(xs) + k + 1, n_lanes=lanes, precision=args.precision)
+                          seed=rank * len(xs) + k + 1, n_lanes=lanes, precision=precision)
                for k in sel]
         ctx.flush()
         ts = [ctx.fetch(j, nb) for j in ids]
@@ -184,11 +217,21 @@ def run_ours(args, rank, world, local_rank, dist):
         sts = [ctx.stats(j) for j in ids]
         for j in ids:
             ctx.release(j)
-        if resident_mid is None:
+        if own:
             ctx.release_mesh(mid)
         wall = (time.perf_counter() - t0) * 1e3
-        dev = sts[0]["device_ms"]
-        return dev, wall, sum(s["packets"] for s in sts), sum(s["steps"] for s in sts), ts, sts
+        launches = {s["launch_id"] for s in sts}
+        if len(launches) != 1:
+            raise RuntimeError(f"a bench step ran in {len(launches)} launches: {sorted(launches)}")
+        return (sts[0]["device_ms"], wall, sum(s["packets"] for s in sts),
+                sum(s["steps"] for s in sts), ts, sts)
+
+    def one_step(mid):
+        """The next batch of A-scans of the B-scan: step k runs positions
+        k*batch .. k*batch+batch-1 (wrapping at the end of the scan)."""
+        sel = step_positions(counter[0], batch, len(xs))
+        counter[0] += 1
+        return run_batch(mid, sel, args.precision)
 
     def barrier():
         if dist is not None:
@@ -198,18 +241,14 @@ def run_ours(args, rank, world, local_rank, dist):
     mid = ctx.upload_mesh(mesh)
     tuned = None
     if args.autotune:
-        # launch variant chosen on 4 A-scans' worth of packets at the first position
-        best, table = ctx.autotune(mid, sim, xs[0], roots[0], precision=args.precision,
-                                   n_photons=args.photons, n_jobs=4, n_lanes=lanes)
-        tuned = {"blocks_per_sm": best[0], "scatter_share": best[1],
-                 "table_steps_per_s": [[b, sh, round(v)] for b, sh, v in table]}
+        tuned = autotune(ctx, mid, sim, xs, roots, args, lanes)
     for _ in range(args.warmup):
         one_step(mid)
     barrier()
     sampler = ClockSampler(local_rank)
     sampler.start()
     dev_ms, packets, steps = 0.0, 0, 0
-    last = None
+    last, first_timed = None, counter[0]
     for _ in range(args.steps):
         flush_buf.fill_(1)  # evict L2 between timed steps
         torch.cuda.synchronize()
@@ -221,94 +260,93 @@ def run_ours(args, rank, world, local_rank, dist):
     barrier()
     # end to end through the C-ABI: upload, submit, run, fetch, per step
     e2e_ms = 0.0
-    for _ in range(max(1, min(args.steps, 2))):
+    e2e_steps = max(1, min(args.steps, 2))
+    for _ in range(e2e_steps):
         flush_buf.fill_(1)
         torch.cuda.synchronize()
-        _, w, p_e, _, _, _ = one_step(None)
+        _, w, _, _, _, _ = one_step(None)
         e2e_ms += w
-    e2e_steps = max(1, min(args.steps, 2))
     barrier()
     clocks = sampler.stop()
 
-    # The same workload one A-scan per launch (submit, run, fetch, next), on
-    # the first A-scans of the scan: the batched launches' gain over the
-    # plain single-job use.  Compared in propagation steps per second (the
-    # A-scans differ in steps per packet).  Untimed for the headline.
-    ctx.configure(linger_us=-1)
-    # End to end, each A-scan also uploads and releases the mesh, as the
-    # reference's per-A-scan worker does (src/main.cu:447-465, 638-658).
-    plain_ms, plain_steps, plain_packets, plain_wall = 0.0, 0, 0, 0.0
-    for k in range(min(args.plain_ascans, len(xs))):
-        t0 = time.perf_counter()
-        mid_k = ctx.upload_mesh(mesh)
-        j = ctx.submit(mid_k, sim, xs[k], roots[k], n_photons=args.photons,
-                       seed=rank * len(xs) + k + 1, n_lanes=lanes, precision=args.precision)
-        ctx.flush()
-        ctx.fetch(j, nb)
-        ctx.synchronize()
-        s = ctx.stats(j)
-        ctx.release(j)
-        ctx.release_mesh(mid_k)
-        plain_wall += time.perf_counter() - t0
-        plain_ms += s["device_ms"]
-        plain_steps += s["steps"]
-        plain_packets += s["packets"]
-    ctx.configure(linger_us=0)
+    # The plain single-job form: one A-scan per launch (submit, run, fetch,
+    # next) on the first A-scans of the scan, each also uploading and
+    # releasing the mesh end to end as the reference's per-A-scan worker does
+    # (src/main.cu:447-465, 638-658).  Compared in propagation steps per
+    # second (A-scans differ in steps per packet).  Untimed for the headline.
     plain = None
-    if plain_ms > 0:
-        batched_sps = steps / (dev_ms / 1e3)
-        plain_sps = plain_steps / (plain_ms / 1e3)
-        plain = {"ascans": min(args.plain_ascans, len(xs)), "packets_per_s": plain_packets / (plain_ms / 1e3),
-                 "propagation_steps_per_s": plain_sps, "batched_over_plain": batched_sps / plain_sps,
-                 "e2e_packets_per_s": plain_packets / plain_wall,
-                 "note": "one A-scan per launch; device time, ratio of propagation steps/s; e2e "
-                         "includes a mesh upload per A-scan as in the reference's worker"}
+    if args.plain_ascans > 0:
+        ctx.configure(linger_us=-1)
+        p_ms, p_steps, p_packets, p_wall = 0.0, 0, 0, 0.0
+        for k in range(min(args.plain_ascans, len(xs))):
+            d, w, p, s, _, _ = run_batch(None, [k], args.precision)
+            p_ms += d
+            p_wall += w
+            p_steps += s
+            p_packets += p
+        ctx.configure(linger_us=0)
+        plain = {"ascans": min(args.plain_ascans, len(xs)),
+                 "packets_per_s": p_packets / (p_ms / 1e3),
+                 "propagation_steps_per_s": p_steps / (p_ms / 1e3),
+                 "batched_over_plain": (steps / (dev_ms / 1e3)) / (p_steps / (p_ms / 1e3)),
+                 "e2e_packets_per_s": p_packets / (p_wall / 1e3),
+                 "note": "one A-scan per launch; device time, ratio of propagation steps/s; "
+                         "e2e includes a mesh upload per A-scan as in the reference's worker"}
+
+    # The FP64 form (the reference's arithmetic) beside the mixed form, on
+    # the same A-scans of the first timed step, one launch each: the
+    # speed-up without the precision change.
+    fp64 = None
+    if args.fp64_ascans > 0 and args.precision == 0:
+        sel = step_positions(first_timed, batch, len(xs))[: args.fp64_ascans]
+        d64, _, p64, s64, _, _ = run_batch(mid, sel, 2)
+        dmx, _, pmx, smx, _, _ = run_batch(mid, sel, 0)
+        fp64 = {"ascans": len(sel), "packets_per_s": p64 / (d64 / 1e3),
+                "propagation_steps_per_s": s64 / (d64 / 1e3),
+                "mixed_packets_per_s_same_ascans": pmx / (dmx / 1e3),
+                "mixed_over_fp64": (smx / (dmx / 1e3)) / (s64 / (d64 / 1e3)),
+                "f_step": F_STEP_FP64,
+                "frac_of_fp64_peak": s64 / (d64 / 1e3) * F_STEP_FP64 /
+                (fp_peak_tflops(clocks, 64) * 1e12)}
 
     t_dev = torch.tensor([dev_ms, e2e_ms / e2e_steps], dtype=torch.float64, device="cuda")
     if dist is not None:
         dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
     dev_ms_max, e2e_ms_step = float(t_dev[0]), float(t_dev[1])
-    total_packets = packets * world
-    value = total_packets / (dev_ms_max / 1e3)
-    ms_per_step = dev_ms_max / args.steps
+    value = packets * world / (dev_ms_max / 1e3)
     e2e_value = (packets // args.steps) * world / (e2e_ms_step / 1e3)
     if plain is not None:
         plain["batched_e2e_over_plain_e2e"] = e2e_value / world / plain["e2e_packets_per_s"]
     ts, sts = last
     rel_peak, rel_mean = rel_error_at_peak(ts[len(ts) // 2], args.photons)
     launch_s = dev_ms / args.steps / 1e3
-    steps_per_launch = steps / args.steps
-    achieved = steps_per_launch * B_STEP / launch_s / 1e9
-    peak, peak_kind = measured_peaks()
+    steps_per_s = steps / args.steps / launch_s
+    f_step = F_STEP[args.precision]
+    peak32 = fp_peak_tflops(clocks, 64 if args.precision == 2 else 32)
+    achieved = steps_per_s * f_step / 1e12
+    hbm_peak, hbm_kind = measured_hbm()
     h2d = mesh.n_tets * 80 + batch * (lanes * 36 + 5 * 4 * sim.n_regions + 48)
     d2h = batch * (tally_bytes(nb, args.precision) + 32)
     ctx.release_mesh(mid)
     ctx.close()
+    cfg = workload_config(args, len(xs), batch, mesh.n_tets)
+    cfg["rng_lanes_per_ascan"] = lanes
+    cfg["parallelism"] = f"weak x{world} (A-scan batches per rank)"
     return {
-        "metric": "photon packets/s (B-scan, 256 A-scans)",
+        "metric": METRIC,
         "value": value,
         "unit": "packets/s",
         "n_gpus": world,
         "impl": "ours",
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": ms_per_step,
+        "ms_per_step": dev_ms_max / args.steps,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": {0: "f32+f64", 1: "f32", 2: "f64"}[args.precision],
         "data": "synthetic",
-        "config": {
-            "workload": f"bscan ellipsoid+2 spheres, {mesh.n_tets} tets, {len(xs)} A-scans x "
-                        f"{args.photons} packets, seeds 1..{len(xs)}; one step = {batch} "
-                        f"A-scans in one launch",
-            "ascans_per_step": batch,
-            "precision": {0: "mixed FP32 geometry / FP64 path+tally", 1: "FP32",
-                          2: "FP64"}[args.precision],
-            "rng_lanes_per_ascan": lanes,
-            "parallelism": f"weak x{world} (A-scan batches per rank)",
-            "l2": "256 MB buffer written between timed steps",
-        },
+        "config": cfg,
         "ascans_per_s": batch * world * args.steps / (dev_ms_max / 1e3),
         "steps_per_packet": steps / packets,
         "propagation_steps_per_s": steps * world / (dev_ms_max / 1e3),
@@ -316,85 +354,136 @@ def run_ours(args, rank, world, local_rank, dist):
                              "ascan": "middle A-scan, last timed step"},
         "e2e": {"value": e2e_value, "unit": "packets/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms_step},
-        "gpu_launches": args.steps * 1,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak,
-                     "traffic": mesh.n_tets * 80 + batch * DRAM_PER_ASCAN,
-                     "traffic_note": "DRAM bytes per launch, modelled from an ncu capture of "
-                                     "8 A-scans x 2e5 packets (mesh once + per-A-scan state); "
-                                     "far below the algorithmic bytes because the mesh is "
-                                     "L2-resident",
-                     "note": f"algorithmic {B_STEP} B per propagation step x steps per launch / "
-                             f"launch time; peak = {peak_kind} HBM copy bandwidth; the mesh "
-                             f"({mesh.n_tets * 80 / 1e6:.0f} MB) is L2-resident, the kernel is "
-                             f"bound by instruction issue and gather latency"},
+        "gpu_launches": args.steps,
+        "roofline": {
+            "bound": "issue", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
+            "frac": achieved / peak32,
+            "traffic": mesh.n_tets * 80 + batch * DRAM_PER_ASCAN,
+            "f_step": f_step,
+            "note": f"algorithmic FLOPs per propagation step (F_step, the oracle's operation "
+                    f"census on this workload: + - x / sqrt 1, FMA 2, transcendental 1) x "
+                    f"steps/s of the photon kernel (CUDA events on its stream); peak = "
+                    f"{'FP64' if args.precision == 2 else 'FP32'} lanes of 148 SMs x 2 x the "
+                    f"median SM clock sampled while timing (no measured non-tensor peak is "
+                    f"provided); the kernel is bound by issue latency and divergence, not "
+                    f"by FLOPs",
+            "traffic_note": "DRAM bytes per launch, modelled from an ncu capture of 8 A-scans "
+                            "x 2e5 packets (mesh once + per-A-scan state); the mesh is "
+                            "L2-resident",
+            "secondary_hbm": {"achieved_gbs": steps_per_s * B_STEP / 1e9, "peak_gbs": hbm_peak,
+                              "frac": steps_per_s * B_STEP / 1e9 / hbm_peak,
+                              "note": f"nominal: {B_STEP} B of planes and neighbours per step "
+                                      f"against the {hbm_kind} HBM copy bandwidth; served "
+                                      f"from L2"},
+        },
         "clocks": clocks,
         "plain_single_job": plain,
+        "fp64": fp64,
         "autotune": tuned,
+        "first_timed_position": first_timed * batch % len(xs),
     }
 
 
-def cpu_sample(args, packets_hint=None, n_threads=0, target_s=12.0):
-    """The reference's own routine on the host: one A-scan of the workload."""
+def reference_inputs(args):
+    """The workload as the reference itself reads it, without the product
+    library: the deck files (meshgen writes input files only), parsed by the
+    reference's read_simulation_data + Bias_Read; the mesh serialised by the
+    reference's own MeshGraph + SerializeGraph and the roots found by its
+    FindRootofGraph (cached by oracle/ref_mesh_cache.py: the O(T^2) builder
+    takes about an hour at 380,928 tets); the multiplier file written by the
+    oracle's generator and read by the reference's init_RNG."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import octmps
     import oracle_py
-    ref = oracle_py.Reference()
+    import ref_mesh_cache
+    ref = oracle_py.Reference(oracle_py.REF_FAST_SO)
     work = tempfile.mkdtemp(prefix="octmps_ref_")
-    sim, mesh, xs, roots = make_workload(argparse.Namespace(ascans=1, photons=args.photons), work)
-    import meshgen  # noqa: F401
-    p = os.path.join(work, "bscan")
-    rs = ref.parse(p + ".opt", p + ".mci")
+    p = ref_mesh_cache.bscan_deck(work, n_photons=args.photons)
+    rs = ref.parse(p["opt"], p["mci"])
+    cache = ref_mesh_cache.load(p["mesh"])
+    mesh = {"tet": cache["tet"], "planes": cache["planes"]}
+    xs = [float(x) for x in cache["xs"]][: args.ascans]
     sp = os.path.join(work, "safeprimes_base32.txt")
-    n_blocks = 8
+    n_blocks = REF_BLOCKS
     lanes = n_blocks * ref.threads_per_block
-    octmps.write_safeprimes(sp, 3 + 3 * lanes)
-    n_threads = n_threads or os.cpu_count()
+    oracle_py.Oracle().write_safeprimes(sp, 3 + 3 * lanes)
+    return ref, rs, mesh, xs, [int(r) for r in cache["roots"]], sp, n_blocks, lanes
 
-    def run(n):
-        rs.number_of_photons = n
-        rng = ref.init_rng(lanes, sp, 1)
-        t = ref.run(rs, mesh, roots[0], (xs[0], 0.0, 0.0), n_blocks, rng, n_threads=n_threads)
-        return t["seconds"]
 
-    n0 = max(lanes * 2, 10000)
-    s0 = run(n0)
-    rate0 = n0 / s0
-    n = packets_hint or int(max(lanes, min(5e7, rate0 * target_s)))
-    return run, n, n_threads, rate0, lanes
+REF_BLOCKS = 2  # reference grid of the CPU runs: 2 blocks x 600 threads = 1,200 lanes
+
+
+def step_positions(k, batch, n):
+    """A-scan positions of bench step k (warm-up steps included): the batch
+    that the GPU arm runs in its k-th launch."""
+    return [(k * batch + j) % n for j in range(batch)]
+
+
+def reference_step(inp, positions, packets, n_threads):
+    """The reference's own per-photon routine (OCTMPSKernel relaunched until
+    its photon counter runs out, src/main.cu:572-623) over the given A-scans,
+    `packets` each, seeds position + 1; returns (packets, seconds of the
+    relaunch loops)."""
+    ref, rs, mesh, xs, roots, sp, n_blocks, lanes = inp
+    rs.number_of_photons = packets
+    secs = 0.0
+    for k in positions:
+        rng = ref.init_rng(lanes, sp, k + 1)
+        t = ref.run(rs, mesh, roots[k], (xs[k], 0.0, 0.0), n_blocks, rng, n_threads=n_threads)
+        secs += t["seconds"]
+    return packets * len(positions), secs
+
+
+def autotune(ctx, mid, sim, xs, roots, args, lanes):
+    """Launch variant chosen on 4 A-scans of the first positions."""
+    best, table = ctx.autotune(mid, sim, xs[0], roots[0], precision=args.precision,
+                               n_photons=args.photons, n_jobs=4, n_lanes=lanes)
+    return {"blocks_per_sm": best[0], "scatter_share": best[1],
+            "table_steps_per_s": [[b, sh, round(v)] for b, sh, v in table]}
 
 
 def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU routine on the host cores, step k
+    running the same A-scan positions as the GPU arm's k-th launch, with a
+    bounded number of packets per A-scan."""
     if rank != 0:
         return None
     try:
-        run, n, threads, rate0, lanes = cpu_sample(args, target_s=8.0)
-    except ImportError as e:
-        return {"impl": "reference", "unavailable": f"reference host build missing: {e}"}
-    for _ in range(args.warmup):
-        run(max(lanes, n // 8))
-    times = [run(n) for _ in range(args.steps)]
-    tot = sum(times)
-    value = n * args.steps / tot
+        inp = reference_inputs(args)
+    except (ImportError, FileNotFoundError, ValueError) as e:
+        return {"impl": "reference", "unavailable": f"reference host build or mesh cache "
+                                                    f"missing: {e}"}
+    threads = os.cpu_count()
+    lanes = inp[7]
+    n_xs = len(inp[3])
+    batch = min(args.batch, n_xs)
+    for k in range(args.warmup):
+        reference_step(inp, step_positions(k, batch, n_xs)[:1], lanes, threads)
+    packets, secs = 0, 0.0
+    for k in range(args.warmup, args.warmup + args.steps):
+        p, t = reference_step(inp, step_positions(k, batch, n_xs), args.ref_packets, threads)
+        packets += p
+        secs += t
+    value = packets / secs
+    sample = (f"{args.ref_packets} packets of each of the {batch} A-scans of each timed GPU step "
+              f"(positions {args.warmup * batch % n_xs}..), {lanes} lanes, seeds position+1")
     return {
         "impl": "reference",
-        "metric": "photon packets/s (B-scan, 256 A-scans)",
+        "metric": METRIC,
         "value": value,
         "unit": "packets/s",
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": tot / args.steps * 1e3,
+        "ms_per_step": secs / args.steps * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "bscan ellipsoid+2 spheres, 380928 tets; sample: 1 A-scan per step",
-                   "lanes": lanes},
+        "config": workload_config(args, n_xs, batch),
         "cpu_baseline": {"value": value, "unit": "packets/s", "cores": threads,
-                         "kind": "reference",
-                         "sample": f"{n} packets of one A-scan per step, {lanes} lanes"},
+                         "kind": "reference", "sample": sample,
+                         "build": "reference sources, g++ -O3 -march=x86-64-v4 -fopenmp"},
         "e2e": {"value": value, "unit": "packets/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -416,6 +505,14 @@ def main():
                     help="choose the launch variant on a sample before timing")
     ap.add_argument("--plain-ascans", type=int, default=4,
                     help="A-scans run one per launch for the batched-over-plain ratio")
+    ap.add_argument("--fp64-ascans", type=int, default=8,
+                    help="A-scans of the first timed step rerun in the FP64 form")
+    ap.add_argument("--cpu-ascans", type=int, default=8,
+                    help="A-scans of the ours-arm cpu_baseline sample")
+    ap.add_argument("--cpu-packets", type=int, default=4800,
+                    help="packets per A-scan of the ours-arm cpu_baseline sample")
+    ap.add_argument("--ref-packets", type=int, default=1200,
+                    help="packets per A-scan of each --impl reference step")
     args = ap.parse_args()
     rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
     local_rank = env_int("LOCAL_RANK", 0)
@@ -437,14 +534,21 @@ def main():
         dist = td
     out = run_ours(args, rank, world, local_rank, dist)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the reference's routine on the host cores, on the A-scans of the
+        # first timed step (a bounded sample, about 10 s)
         try:
-            run, n, threads, rate0, lanes = cpu_sample(args, target_s=12.0)
-            secs = run(n)
-            out["cpu_baseline"] = {"value": n / secs, "unit": "packets/s", "cores": threads,
-                                   "kind": "reference",
-                                   "sample": f"{n} packets of one A-scan of the workload "
-                                             f"({lanes} lanes), reference routine compiled for "
-                                             f"the host with OpenMP"}
+            inp = reference_inputs(args)
+            n_xs = len(inp[3])
+            batch = min(args.batch, n_xs)
+            sel = step_positions(args.warmup, batch, n_xs)[: args.cpu_ascans]
+            threads = os.cpu_count()
+            p, secs = reference_step(inp, sel, args.cpu_packets, threads)
+            out["cpu_baseline"] = {
+                "value": p / secs, "unit": "packets/s", "cores": threads, "kind": "reference",
+                "sample": f"{args.cpu_packets} packets of each of {len(sel)} A-scans of the first "
+                          f"timed step (positions {sel[0]}..{sel[-1]}), {inp[7]} lanes, "
+                          f"reference routine built -O3 -march=x86-64-v4 -fopenmp, mesh from the "
+                          f"reference's own MeshGraph"}
         except Exception as e:  # the baseline never hides the GPU result
             out["cpu_baseline"] = {"value": None, "unit": "packets/s", "cores": os.cpu_count(),
                                    "kind": "reference", "sample": f"unavailable: {e}"}

@@ -338,6 +338,18 @@ typedef struct {
 } octmps_noalloc_ascan;
 octmps_status octmps_ascan_run_noalloc(const octmps_noalloc_ascan *a, void *stream);
 
+/* ---- A-scans of a B-scan ---------------------------------------------------
+ * octmps_probe_positions: the probe positions of main()'s A-scan loop
+ * (src/main.cu:948-950), x from start_x while x < end_x in double steps of
+ * step_x; writes at most max_out, returns the count (-1: invalid).
+ * octmps_ascans_of_gpu: the A-scans GPU `gpu` of `n_gpus` runs under the
+ * CLI's -G (round robin: gpu, gpu + n_gpus, ...); replaces the per-GPU photon
+ * split of DoOneSimulation (src/main.cu:665-848); writes at most max_out
+ * indices, returns the count (-1: invalid). */
+int64_t octmps_probe_positions(const octmps_sim *sim, double *out, uint64_t max_out);
+int64_t octmps_ascans_of_gpu(uint64_t n_ascans, uint32_t n_gpus, uint32_t gpu, uint64_t *out,
+                             uint64_t max_out);
+
 /* ---- multiplier table generation (safeprimes_base32.txt) ---------------- */
 int octmps_safeprimes_generate(uint32_t *out, uint64_t count);
 int octmps_safeprimes_write(const char *path, uint64_t count);

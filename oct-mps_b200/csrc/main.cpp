@@ -129,8 +129,13 @@ int main(int argc, char **argv) {
 
     octmps_mesh_desc md{hm.n_tets, hm.n_faces, hm.tet_region, hm.tet_faces,
                         hm.tet_signs, hm.tet_adj, hm.face_plane};
-    std::vector<double> xs;
-    for (double x = sim.start_x; x < sim.end_x; x += sim.step_x) xs.push_back(x);
+    const int64_t n_xs = octmps_probe_positions(&sim, nullptr, 0);
+    if (n_xs < 0) {
+        printf("Something wrong with the probe scan parameters!\n");
+        return 1;
+    }
+    std::vector<double> xs((size_t)n_xs);
+    octmps_probe_positions(&sim, xs.data(), xs.size());
     std::vector<int32_t> roots(xs.size());
     for (size_t k = 0; k < xs.size(); ++k) {
         if (octmps_mesh_find_root(&md, xs[k], 0.0, 0.0, &roots[k]) != OCTMPS_OK) {
@@ -178,16 +183,19 @@ int main(int argc, char **argv) {
     std::vector<std::thread> threads;
     for (unsigned int g = 0; g < ngpu; ++g) {
         threads.emplace_back([&, g]() {
+            std::vector<uint64_t> mine(xs.size());
+            mine.resize((size_t)octmps_ascans_of_gpu(xs.size(), ngpu, g, mine.data(), mine.size()));
             octmps_ctx *ctx = nullptr;
             if (octmps_ctx_create((int)g, &ctx) != OCTMPS_OK) {
-                for (size_t k = g; k < xs.size(); k += ngpu) res[k].st = OCTMPS_ERR_NO_DEVICE;
+                for (uint64_t k : mine) res[k].st = OCTMPS_ERR_NO_DEVICE;
                 return;
             }
             octmps_ctx_set_multipliers(ctx, mult.data(), mult.size());
             octmps_mesh_id mid = 0;
             octmps_status st = octmps_mesh_upload(ctx, &md, &mid);
             std::vector<octmps_job_id> ids(xs.size(), 0);
-            for (size_t k = g; k < xs.size() && st == OCTMPS_OK; k += ngpu) {
+            for (uint64_t k : mine) {
+                if (st != OCTMPS_OK) break;
                 octmps_job jb;
                 memset(&jb, 0, sizeof jb);
                 jb.mesh = mid;
@@ -201,7 +209,7 @@ int main(int argc, char **argv) {
                 st = octmps_job_submit(ctx, &jb, &ids[k]);
                 if (st != OCTMPS_OK) fprintf(stderr, "[GPU %u] %s\n", g, octmps_last_error(ctx));
             }
-            for (size_t k = g; k < xs.size(); k += ngpu) {
+            for (uint64_t k : mine) {
                 if (st != OCTMPS_OK) {
                     res[k].st = st;
                     continue;

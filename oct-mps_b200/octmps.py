@@ -136,6 +136,7 @@ EXPORTED = [
     "octmps_job_fetch", "octmps_job_fetch_stats", "octmps_job_release", "octmps_read_opt",
     "octmps_read_mci", "octmps_write_result", "octmps_safeprimes_generate",
     "octmps_safeprimes_write", "octmps_safeprimes_read", "octmps_ascan_run_noalloc",
+    "octmps_probe_positions", "octmps_ascans_of_gpu",
 ]
 
 _lib = None
@@ -180,6 +181,9 @@ def lib():
             "octmps_safeprimes_write": (C.c_int, [C.c_char_p, C.c_uint64]),
             "octmps_safeprimes_read": (C.c_int64, [C.c_char_p, P(C.c_uint32), C.c_uint64]),
             "octmps_debug_record_next_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
+            "octmps_probe_positions": (C.c_int64, [P(Sim), P(C.c_double), C.c_uint64]),
+            "octmps_ascans_of_gpu": (C.c_int64, [C.c_uint64, C.c_uint32, C.c_uint32,
+                                                 P(C.c_uint64), C.c_uint64]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -218,12 +222,22 @@ def read_deck(opt_path, mci_path):
 
 def probe_positions(sim):
     """The A-scan loop of main (src/main.cu:948-950), in the same double steps."""
-    xs = []
-    x = sim.start_x
-    while x < sim.end_x:
-        xs.append(x)
-        x += sim.step_x
-    return xs
+    n = lib().octmps_probe_positions(C.byref(sim), None, 0)
+    if n < 0:
+        raise OctmpsError(1, "probe scan never ends (step_x <= 0)")
+    out = np.zeros(n, np.float64)
+    lib().octmps_probe_positions(C.byref(sim), _ptr(out, C.c_double), n)
+    return out.tolist()
+
+
+def ascans_of_gpu(n_ascans, n_gpus, gpu):
+    """A-scans GPU `gpu` of `n_gpus` runs under the CLI's -G (round robin)."""
+    n = lib().octmps_ascans_of_gpu(n_ascans, n_gpus, gpu, None, 0)
+    if n < 0:
+        raise OctmpsError(1, f"invalid split: gpu {gpu} of {n_gpus}")
+    out = np.zeros(n, np.uint64)
+    lib().octmps_ascans_of_gpu(n_ascans, n_gpus, gpu, _ptr(out, C.c_uint64), n)
+    return [int(k) for k in out]
 
 
 class Mesh:

@@ -248,7 +248,9 @@ inline T rand_oc(uint64_t *x, uint32_t a) {
 // accurate formulations of the same quantities; the FP64 form keeps the
 // reference's operations.
 template <typename T>
-constexpr bool kFused = std::is_same<T, float>::value;
+struct FusedForm : std::is_same<T, float> {};
+template <typename T>
+constexpr bool kFused = FusedForm<T>::value;
 
 // a.x + b.y + c.z evaluated left to right, (a.x + b.y) + c.z, as the
 // reference writes its dot products; fused in the FP32 forms.
@@ -767,9 +769,10 @@ struct Lane {
                 if (dump && k == dump_packet && r.steps < dump_max) {
                     dump_rows = r.steps + 1;
                     double *d = dump + 12 * (size_t)r.steps;
-                    d[0] = ph.tet; d[1] = ev; d[2] = ph.x; d[3] = ph.y; d[4] = ph.z;
-                    d[5] = ph.ux; d[6] = ph.uy; d[7] = ph.uz; d[8] = ph.w;
-                    d[9] = ph.s; d[10] = (double)ph.optical_path; d[11] = ph.lr;
+                    d[0] = ph.tet; d[1] = ev; d[2] = (double)ph.x; d[3] = (double)ph.y;
+                    d[4] = (double)ph.z; d[5] = (double)ph.ux; d[6] = (double)ph.uy;
+                    d[7] = (double)ph.uz; d[8] = (double)ph.w; d[9] = (double)ph.s;
+                    d[10] = (double)ph.optical_path; d[11] = (double)ph.lr;
                 }
                 r.steps++;
                 ++steps;
@@ -969,6 +972,76 @@ int oracle_dump_lane(const OracleParams *p, const OracleMesh *m, double probe_x,
                                               xS, aS, out, max_steps, packet_index);
     }
     return -1;
+}
+
+// Multiplier list of the MWC generators, for runs that must not load the
+// product library (the bench's reference arm).  The reference reads the
+// first column of safeprimes_base32.txt (src/octmps_kernel.cuh:74-105), a
+// file it does not ship; a valid multiplier a < 2^32 makes a*2^32 - 1 and
+// a*2^31 - 1 both prime.  The list is every such a in descending order from
+// 2^32 - 1, found by trial division by the odd primes below 100 and the
+// deterministic 64-bit Miller-Rabin test (bases 2, 325, 9375, 28178, 450775,
+// 9780504, 1795265022, after J. Sinclair).  Returns 0 when `count` entries
+// were written.
+namespace {
+typedef unsigned __int128 u128;
+uint64_t mr_pow(uint64_t b, uint64_t e, uint64_t m) {
+    uint64_t r = 1;
+    b %= m;
+    for (; e; e >>= 1) {
+        if (e & 1) r = (uint64_t)((u128)r * b % m);
+        b = (uint64_t)((u128)b * b % m);
+    }
+    return r;
+}
+bool mr_prime(uint64_t n) {
+    static const uint64_t small[] = {3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47,
+                                     53, 59, 61, 67, 71, 73, 79, 83, 89, 97};
+    if (n < 2) return false;
+    if (n % 2 == 0) return n == 2;
+    for (uint64_t q : small)
+        if (n % q == 0) return n == q;
+    uint64_t d = n - 1;
+    int r = 0;
+    while (!(d & 1)) { d >>= 1; ++r; }
+    for (uint64_t a : {2ull, 325ull, 9375ull, 28178ull, 450775ull, 9780504ull, 1795265022ull}) {
+        uint64_t x = mr_pow(a, d, n);
+        if (x == 0 || x == 1 || x == n - 1) continue;
+        bool comp = true;
+        for (int i = 1; i < r && comp; ++i) {
+            x = (uint64_t)((u128)x * x % n);
+            if (x == n - 1) comp = false;
+        }
+        if (comp) return false;
+    }
+    return true;
+}
+}  // namespace
+
+int oracle_safeprimes(uint32_t *out, uint64_t count) {
+    const uint64_t chunk = 1 << 16;
+    uint64_t found = 0, top = 0xffffffffull;
+    while (found < count && top >= 0x80000000ull) {
+        const int nchunks = 64;
+        std::vector<std::vector<uint32_t>> got(nchunks);
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int c = 0; c < nchunks; ++c) {
+            const uint64_t hi = top - (uint64_t)c * chunk;
+            for (uint64_t i = 0; i < chunk; ++i) {
+                const uint64_t a = hi - i;
+                if (a < 0x80000000ull) break;
+                if (mr_prime((a << 31) - 1) && mr_prime((a << 32) - 1))
+                    got[c].push_back((uint32_t)a);
+            }
+        }
+        for (int c = 0; c < nchunks && found < count; ++c)
+            for (uint32_t a : got[c]) {
+                if (found == count) break;
+                out[found++] = a;
+            }
+        top = top >= (uint64_t)nchunks * chunk ? top - (uint64_t)nchunks * chunk : 0;
+    }
+    return found == count ? 0 : 1;
 }
 
 float oracle_logf(float x) { return logf_method(x); }

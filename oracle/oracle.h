@@ -119,6 +119,11 @@ void oracle_sincos_d(double psi, double *s, double *c);
 double oracle_div_rd(double a, double b);
 float oracle_uint2float_rz(uint32_t u);
 
+/* MWC multiplier list: every a < 2^32 with a*2^32 - 1 and a*2^31 - 1 prime,
+ * descending from 2^32 - 1 (the first column of the reference's missing
+ * safeprimes_base32.txt, src/octmps_kernel.cuh:74-105).  0 on success. */
+int oracle_safeprimes(uint32_t *out, uint64_t count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,7 +16,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "liboctmps_oracle.so")
+CENSUS_SO = os.path.join(HERE, "_build", "liboctmps_census.so")
+CENSUS_FIELDS = ("add", "mul", "div", "sqrt", "fma", "trans")
 REF_SO = os.path.join(HERE, "_ref", "libocref.so")
+# the same sources built -O3 -march=x86-64-v4 with contraction: the timed CPU baseline
+REF_FAST_SO = os.path.join(HERE, "_ref", "libocref_fast.so")
 MAX_REGIONS = 100
 
 P = C.POINTER
@@ -159,9 +163,26 @@ class Oracle:
         L.oracle_sincos_d.argtypes = [C.c_double, P(C.c_double), P(C.c_double)]
         L.oracle_div_rd.restype = C.c_double
         L.oracle_div_rd.argtypes = [C.c_double, C.c_double]
+        L.oracle_safeprimes.restype = C.c_int
+        L.oracle_safeprimes.argtypes = [P(C.c_uint32), C.c_uint64]
         L.oracle_uint2float_rz.restype = C.c_float
         L.oracle_uint2float_rz.argtypes = [C.c_uint32]
         self.L = L
+
+    def safeprimes(self, count):
+        """The MWC multiplier list (first column of safeprimes_base32.txt)."""
+        out = np.zeros(count, np.uint32)
+        if self.L.oracle_safeprimes(_ptr(out, C.c_uint32), count) != 0:
+            raise RuntimeError("multiplier list too short")
+        return out
+
+    def write_safeprimes(self, path, count):
+        """safeprimes_base32.txt with `count` rows: a, then the high and low
+        32-bit words of a*2^32 - 1 (the reference reads the first column)."""
+        a = self.safeprimes(count)
+        with open(path, "w") as f:
+            for v in a.tolist():
+                f.write(f"{v} {v - 1} {0xffffffff}\n")
 
     @staticmethod
     def _mesh(mesh):
@@ -306,6 +327,16 @@ class Reference:
 
     @staticmethod
     def mesh_struct(mesh, root):
+        """RefMesh of a mesh: an object with region/faces/signs/adj/planes
+        arrays, or a dict {"tet": (T, 14) serialised tets, "planes": (F, 4)}
+        as SerializeGraph writes them."""
+        if isinstance(mesh, dict):
+            tet = np.ascontiguousarray(mesh["tet"], np.int32)
+            planes = np.ascontiguousarray(mesh["planes"], np.float64)
+            m = RefMesh(len(tet), len(planes), root, _ptr(tet, C.c_int32),
+                        _ptr(planes, C.c_double))
+            m._keep = (tet, planes)
+            return m
         T = len(mesh.region)
         tet = np.zeros((T, 14), np.int32)
         tet[:, 0] = np.arange(T)
@@ -321,7 +352,7 @@ class Reference:
 
     def run(self, sim, mesh, root, probe, n_blocks, rng, n_threads=0):
         """One A-scan through OCTMPSKernel with n_blocks*600 lanes; rng is
-        modified in place (it is the lanes' state)."""
+        modified in place (it is the lanes' state).  mesh: see mesh_struct."""
         m = self.mesh_struct(mesh, root)
         nb = sim.num_optical_depth_length_steps
         t = empty_tally(nb)
@@ -365,3 +396,42 @@ class Reference:
         ts.num_filtered_class1 = int(t["num_filtered_class1"])
         ts.num_filtered_class2 = int(t["num_filtered_class2"])
         self.L.ref_write_result(C.byref(sim), probe_x, C.byref(ts))
+
+
+def census(params, mesh, probe, root, n_photons, n_lanes, rng, precision=0):
+    """Floating-point operations of one A-scan of the oracle's method, counted
+    as they execute (census.cpp), on one thread.  Returns (tally, counts) with
+    counts {"fp32": {...}, "fp64": {...}, "flops": ..., "flops_per_step": ...}:
+    + - x / sqrt 1 each, fused multiply-add 2, transcendental 1."""
+    if not os.path.exists(CENSUS_SO):
+        raise ImportError(f"{CENSUS_SO} not built; run make in {HERE}")
+    L = C.CDLL(CENSUS_SO)
+    L.census_run.restype = C.c_int
+    L.census_run.argtypes = [P(OracleParams), P(OracleMesh), C.c_double, C.c_double, C.c_double,
+                             C.c_int32, C.c_uint64, C.c_uint32, P(C.c_uint64), P(C.c_uint32),
+                             P(C.c_uint64), P(C.c_uint32), P(C.c_uint64), P(C.c_uint32), C.c_int,
+                             P(OracleTally), P(C.c_uint64)]
+    t = empty_tally(params.nbins)
+    ts = _fill_tally_struct(OracleTally, t)
+    out = np.zeros(12, np.uint64)
+    st = L.census_run(C.byref(params), C.byref(Oracle._mesh(mesh)), probe[0], probe[1], probe[2],
+                      root, n_photons, n_lanes, _ptr(rng["x"], C.c_uint64),
+                      _ptr(rng["a"], C.c_uint32), _ptr(rng["xR"], C.c_uint64),
+                      _ptr(rng["aR"], C.c_uint32), _ptr(rng["xS"], C.c_uint64),
+                      _ptr(rng["aS"], C.c_uint32), precision, C.byref(ts), _ptr(out, C.c_uint64))
+    if st != 0:
+        raise RuntimeError(f"census_run failed: {st}")
+    for k in ("num_filtered", "num_filtered_class1", "num_filtered_class2", "steps",
+              "restores", "packets", "capped"):
+        t[k] = getattr(ts, k)
+    counts = {"fp32": dict(zip(CENSUS_FIELDS, (int(v) for v in out[:6]))),
+              "fp64": dict(zip(CENSUS_FIELDS, (int(v) for v in out[6:])))}
+    flops = sum(c["add"] + c["mul"] + c["div"] + c["sqrt"] + 2 * c["fma"] + c["trans"]
+                for c in counts.values())
+    counts["flops"] = flops
+    counts["flops_per_step"] = flops / max(t["steps"], 1)
+    for k in ("fp32", "fp64"):
+        c = counts[k]
+        counts[k + "_flops_per_step"] = (c["add"] + c["mul"] + c["div"] + c["sqrt"] +
+                                         2 * c["fma"] + c["trans"]) / max(t["steps"], 1)
+    return t, counts

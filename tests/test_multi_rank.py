@@ -98,3 +98,20 @@ def test_partition_covers_every_ascan_once():
             flat = sorted(k for p in parts for k in p)
             assert flat == list(range(n))
             assert max(map(len, parts)) - min(map(len, parts)) <= 1
+
+
+def test_cli_gpu_split_matches_the_rank_split(octmps):
+    """The CLI's -G split of A-scans over GPUs (octmps_ascans_of_gpu, which
+    csrc/main.cpp calls per GPU thread) is the multi-rank driver's split:
+    every A-scan exactly once, round robin, sizes within one."""
+    sys.path.insert(0, os.path.join(ROOT, "oct-mps_b200"))
+    import bscan
+    for n in (0, 1, 5, 256, 1000):
+        for g in (1, 2, 3, 4, 8):
+            parts = [octmps.ascans_of_gpu(n, g, r) for r in range(g)]
+            assert parts == [bscan.my_ascans(n, g, r) for r in range(g)]
+            assert sorted(k for p in parts for k in p) == list(range(n))
+    for bad in ((10, 0, 0), (10, 2, 2)):
+        with pytest.raises(octmps.OctmpsError):
+            octmps.ascans_of_gpu(*bad)
+

@@ -187,3 +187,38 @@ def test_oracle_fp32_forms_keep_the_likelihood_finite(octmps, oracle, multiplier
     assert t["num_filtered"] > 0
     for k in ("sum1", "sumsq1", "sum2", "sumsq2"):
         assert np.all(np.isfinite(t[k][:nb])), k
+
+
+def test_oracle_multiplier_list_equals_the_product_generator(oracle, octmps):
+    """The oracle's MWC multiplier list (used where the product library must
+    not be loaded) equals the product's generator entry for entry."""
+    n = 3 + 3 * 2000
+    np.testing.assert_array_equal(oracle.safeprimes(n), octmps.safeprimes(n))
+
+
+def test_operation_census_runs_the_oracle_and_matches_the_frozen_f_step(octmps, meshgen,
+                                                                        workdir):
+    """The census (the oracle's code with counting number types) gives the
+    oracle's tally bit for bit, and its FLOPs per propagation step on a sample
+    of the B-scan workload agree with the value the bench's roofline uses."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    p = meshgen.config_bscan(os.path.join(workdir, "bscan_census"))
+    sim = octmps.read_deck(p["opt"], p["mci"])
+    mesh = octmps.build_mesh(p["mesh"])
+    x = octmps.probe_positions(sim)[128]
+    root = mesh.find_root(x)
+    par = oracle_py.params_from_sim(sim)
+    lanes = 200
+    mult = octmps.safeprimes(3 + 3 * lanes)
+    for prec in (0, 2):
+        t_c, counts = oracle_py.census(par, mesh, (x, 0, 0), root, 2 * lanes, lanes,
+                                       octmps.rng_init(mult, lanes, 129), prec)
+        t_o = oracle_py.Oracle().run(par, mesh, (x, 0, 0), root, 2 * lanes, lanes,
+                                     octmps.rng_init(mult, lanes, 129), prec, n_threads=1)
+        assert t_c["steps"] == t_o["steps"]
+        for k in ("count1", "count2", "sum1", "sumsq1", "sum2", "sumsq2"):
+            np.testing.assert_array_equal(t_c[k], t_o[k], err_msg=k)
+        assert abs(counts["flops_per_step"] / bench.F_STEP[prec] - 1) < 0.02, counts
+
