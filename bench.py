@@ -434,11 +434,12 @@ def reference_step(inp, positions, packets, n_threads):
 
 
 def autotune(ctx, mid, sim, xs, roots, args, lanes):
-    """Launch variant chosen on 4 A-scans of the first positions."""
+    """Launch variant (kernel form, blocks per SM, scatter share) chosen on 4
+    A-scans of the first position."""
     best, table = ctx.autotune(mid, sim, xs[0], roots[0], precision=args.precision,
                                n_photons=args.photons, n_jobs=4, n_lanes=lanes)
-    return {"blocks_per_sm": best[0], "scatter_share": best[1],
-            "table_steps_per_s": [[b, sh, round(v)] for b, sh, v in table]}
+    return {"kernel_form": best[0], "blocks_per_sm": best[1], "scatter_share": best[2],
+            "table_steps_per_s": [[f, b, sh, round(v)] for f, b, sh, v in table]}
 
 
 def run_reference(args, rank, world):

@@ -187,21 +187,32 @@ const char *octmps_status_string(octmps_status st);
  * job is submitted; at least 3 + 3*n_lanes entries. */
 octmps_status octmps_ctx_set_multipliers(octmps_ctx *ctx, const uint32_t *a, uint64_t count);
 
-/* Launch configuration (0 = autotuned / default). */
+/* Launch configuration (0 = default).  Two forms of the photon kernel run
+ * the same per-photon arithmetic:
+ *   pooled (kernel_form 0, the default): 128-thread blocks; each warp holds
+ *     two photons per lane in shared memory and runs every half of a
+ *     propagation step (boundary test, or scattering) on a full warp of
+ *     photons at once;
+ *   per-lane (kernel_form 1): 256-thread blocks, one photon per thread, a
+ *     warp vote choosing which half its lanes run. */
 typedef struct {
-    int32_t block_size;       /* threads per block */
-    int32_t blocks_per_sm;    /* resident 256-thread blocks per SM: 2, 3 or 4 (0 = 3);
-                                 the FP64 form always runs 2 */
+    int32_t block_size;       /* 0, or the form's block size (128 pooled, 256 per-lane) */
+    int32_t blocks_per_sm;    /* resident blocks per SM: pooled 4, 5 or 6 (0 = 5; the FP64
+                                 form 2 or 3, 0 = 2); per-lane 2, 3 or 4 (0 = 3; FP64 2) */
     int32_t default_lanes;    /* RNG lanes per job when job.n_lanes = 0 */
     int32_t use_graphs;       /* reserved, 0 (a batch is one persistent launch, so
                                  there is no launch sequence to replay) */
     uint64_t hbm_budget_bytes;/* admission budget for job state; 0 = 80% of free */
-    int32_t scatter_share;    /* a warp runs its lanes' scattering step halves once at
-                                 least scatter_share/32 of its live lanes wait for one
-                                 (1..32; 0 = 12) */
+    int32_t scatter_share;    /* per-lane: a warp runs its lanes' scattering step halves
+                                 once at least scatter_share/32 of its live lanes wait for
+                                 one; pooled: with fewer than 32 photons waiting for the
+                                 boundary half, the scattering half runs once it holds at
+                                 least scatter_share/32 of the warp's photons (1..32;
+                                 0 = 12) */
     int32_t linger_us;        /* a kernel thread that finds no work waits this long for
                                  newly submitted jobs before it exits (0 = 2000;
                                  -1 = exit at once; at most 1000000) */
+    int32_t kernel_form;      /* 0 pooled (default), 1 per-lane */
 } octmps_launch_config;
 octmps_status octmps_ctx_configure(octmps_ctx *ctx, const octmps_launch_config *cfg);
 

@@ -160,6 +160,21 @@ int launch_photon_kernel(int precision, int min_blocks, const LaunchArgs &args, 
 int photon_kernel_attributes(int precision, int block, int min_blocks, int *regs,
                              int *max_blocks_per_sm);
 
+// Pooled kernel (photon_kernel.cu): 128-thread blocks, each warp holding
+// kPooledPerThread photons per lane in shared memory; min_blocks 4, 5 or 6
+// (FP32 geometry forms), 2 or 3 (FP64 form); the recording variant runs 2.
+// `splits`: a device buffer of pooled_split_bytes(precision, grid) bytes for
+// the photons' split copies, private to the launch.
+constexpr int kPooledBlock = 128;
+constexpr int kPooledPerThread = 2;
+constexpr int kDefaultPooledMinBlocks = 5;
+constexpr int kDefaultPooledMinBlocksFP64 = 2;
+size_t pooled_split_bytes(int precision, int grid);
+int launch_pooled_kernel(int precision, int min_blocks, const LaunchArgs &args, int grid,
+                         void *stream, void *records, void *splits);
+int pooled_kernel_attributes(int precision, int min_blocks, bool record, int *regs,
+                             int *max_blocks_per_sm);
+
 }  // namespace octmps
 
 #endif

@@ -210,8 +210,8 @@ __device__ __noinline__ int tally_detection(const JobDesc *jd, P op, T max_depth
 
 template <typename T, typename P, bool kRecord>
 struct Lane {
-    // photon
-    T x, y, z, ux, uy, uz, w, s, sleft, max_depth, lr, lr_after, loc_fst;
+    // photon (s_next: the step size drawn ahead for the next step, pooled kernel)
+    T x, y, z, ux, uy, uz, w, s, sleft, max_depth, lr, lr_after, loc_fst, s_next;
     P op;
     int32_t tet, region;
     uint32_t fst_flag, num_back;
@@ -442,12 +442,27 @@ struct Lane {
     // when a face is reached, reflection or transmission and the roulette.
     // Returns kDone, kEnd (the packet ended) or kPending (no face reached:
     // the step continues in phase_b).
+    // ComputeStepSize's draw for a step that starts with sleft == 0,
+    // src/octmps_kernel.cuh:505-515.  The pooled kernel draws it at the end
+    // of the previous step (after its roulette and stop checks) or at the
+    // launch: the general stream's draws keep their order, and the first half
+    // of a step no longer diverges on the logarithm.
+    __device__ __forceinline__ void draw_step() {
+        const T r = (T)1 - rand_co_G();
+        s_next = -log_method(r) * rg.rmuas;
+    }
+
+    template <bool kDrawnAhead = false>
     __device__ __forceinline__ int phase_a(SplitCopy<T, P> &cont, unsigned int *err) {
         int ev = 0;
         // ComputeStepSize, :505-515
         if (sleft == (T)0) {
-            const T r = (T)1 - rand_co_G();
-            s = -log_method(r) * rg.rmuas;
+            if (kDrawnAhead) {
+                s = s_next;
+            } else {
+                const T r = (T)1 - rand_co_G();
+                s = -log_method(r) * rg.rmuas;
+            }
         } else {
             s = sleft * rg.rmuas;
             sleft = 0;
@@ -929,6 +944,544 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     }
 }
 
+
+// ------------------------------------------------------------------------
+// Pooled kernel: photons held in shared memory, phases run in full warps.
+//
+// Each warp keeps up to kPool photons (two per lane) in its own slice of
+// shared memory, as two stacks: photons whose next step starts with the
+// boundary test (stack A, positions [0, nA)) and photons that reached no
+// face and wait for their scattering half (stack B, positions
+// [kPool - nB, kPool)).  Every iteration the warp pops up to 32 photons of
+// one stack (B once it holds a full warp's worth, else the fuller one), runs
+// that half of a step on all of them at once, and pushes each result onto
+// the stack of its next half.  Both halves thus run with (nearly) every lane
+// busy, where one photon per thread left a warp's lanes split between the
+// halves.  A photon's arithmetic is that of the per-lane kernel above, step
+// for step: only which lane runs it changes.  The step size of a step that
+// starts with sleft == 0 is drawn at the end of the previous step (after its
+// roulette and stop checks) or at the launch, which keeps the general
+// stream's draws in order and takes the logarithm out of the boundary half.
+//
+// A photon's state is 16-byte chunks (8 for the mixed and FP32 forms, 16 for
+// FP64 and the recording variant); chunk k of the photon at position q sits
+// at chunk (k ^ (q & 7)) of its record, so that 8 consecutive photons read or
+// write a given chunk through 8 different bank groups.  Split copies live
+// in global memory, one per photon identity ("home") of the warp, which a
+// photon keeps across its packets and units.
+
+constexpr int kPoolBlock = 128;  // threads (4 warps) per block
+constexpr int kPoolWarps = kPoolBlock / 32;
+constexpr int kPool = 64;        // photons per warp
+
+// Word layout of a pooled photon (32-bit words; t = words per geometry value):
+//   [0, 13t)        x y z ux uy uz w sleft s_next max_depth lr lr_after loc_fst
+//   META + 0..10    tet | region << 24, flags, num_back, steps of the packet,
+//                   packets left (the current one included), job slot, RNG
+//                   lane, home, aG, aR, aS
+//   OP, XG, XR, XS  optical path (P), generator states (2 words each)
+//   REC             recording variant: hash (2), steps, hits, scatters,
+//                   restores, detections, survivals, contribution (2)
+// flags: bit 31 fst_flag, bit 30 the packet is recorded, bits 0-29 stall.
+template <typename T, typename P, bool kRecord>
+struct PoolLayout {
+    static constexpr int t = (int)(sizeof(T) / 4);
+    static constexpr int META = 13 * t;
+    static constexpr int OP = META + 11;
+    static constexpr int XG = OP + 2, XR = XG + 2, XS = XR + 2;
+    static constexpr int REC = XS + 2;
+    static constexpr int WORDS = REC + (kRecord ? 10 : 0);
+    static constexpr int USED = (WORDS + 3) / 4;           // 16-byte chunks in use
+    static constexpr int CHUNKS = USED <= 8 ? 8 : 16;      // record stride (power of two)
+    static constexpr int PADDED = 4 * USED;
+    static_assert(USED <= 16, "a pooled photon is at most 16 chunks");
+};
+
+static_assert(PoolLayout<float, double, false>::CHUNKS == 8, "mixed form: 8 chunks");
+static_assert(PoolLayout<float, float, false>::CHUNKS == 8, "FP32 form: 8 chunks");
+
+constexpr uint32_t kFlagFst = 1u << 31;
+constexpr uint32_t kFlagRec = 1u << 30;
+constexpr uint32_t kStallMask = (1u << 30) - 1u;
+
+// Per-photon fields kept beside the lane's registers while a half-step runs.
+struct PoolMeta {
+    int32_t slot;
+    uint32_t lane, home, packets_left, steps_packet, flags;
+    uint32_t aG, aR, aS;
+};
+
+__device__ __forceinline__ void put_w(uint32_t *w, int i, float v) { w[i] = __float_as_uint(v); }
+__device__ __forceinline__ void put_w(uint32_t *w, int i, double v) {
+    w[i] = (uint32_t)__double2loint(v);
+    w[i + 1] = (uint32_t)__double2hiint(v);
+}
+__device__ __forceinline__ void put_w(uint32_t *w, int i, unsigned long long v) {
+    w[i] = (uint32_t)v;
+    w[i + 1] = (uint32_t)(v >> 32);
+}
+template <typename F>
+__device__ __forceinline__ F get_w(const uint32_t *w, int i);
+template <>
+__device__ __forceinline__ float get_w<float>(const uint32_t *w, int i) { return __uint_as_float(w[i]); }
+template <>
+__device__ __forceinline__ double get_w<double>(const uint32_t *w, int i) {
+    return __hiloint2double((int)w[i + 1], (int)w[i]);
+}
+template <>
+__device__ __forceinline__ unsigned long long get_w<unsigned long long>(const uint32_t *w, int i) {
+    return (unsigned long long)w[i] | ((unsigned long long)w[i + 1] << 32);
+}
+
+// Chunk k of the photon at position q is chunk (k ^ (q & 7)) of its record.
+template <typename Lay>
+__device__ __forceinline__ void pool_read(const float4 *pool, int q, uint32_t (&w)[Lay::PADDED]) {
+#pragma unroll
+    for (int k = 0; k < Lay::USED; ++k) {
+        const float4 c = pool[q * Lay::CHUNKS + (k ^ (q & 7))];
+        w[4 * k + 0] = __float_as_uint(c.x);
+        w[4 * k + 1] = __float_as_uint(c.y);
+        w[4 * k + 2] = __float_as_uint(c.z);
+        w[4 * k + 3] = __float_as_uint(c.w);
+    }
+}
+
+template <typename Lay>
+__device__ __forceinline__ void pool_write(float4 *pool, int q, const uint32_t (&w)[Lay::PADDED]) {
+#pragma unroll
+    for (int k = 0; k < Lay::USED; ++k)
+        pool[q * Lay::CHUNKS + (k ^ (q & 7))] =
+            make_float4(__uint_as_float(w[4 * k + 0]), __uint_as_float(w[4 * k + 1]),
+                        __uint_as_float(w[4 * k + 2]), __uint_as_float(w[4 * k + 3]));
+}
+
+// The lane's registers (and the job's constants) from a pooled photon.
+template <typename T, typename P, bool kRecord>
+__device__ __forceinline__ void unpack(const uint32_t *w, const LaunchArgs &args, PoolMeta &m,
+                                       Lane<T, P, kRecord> &L) {
+    using Lay = PoolLayout<T, P, kRecord>;
+    constexpr int t = Lay::t, M = Lay::META;
+    m.slot = (int32_t)w[M + 5];
+    m.lane = w[M + 6];
+    m.home = w[M + 7];
+    m.packets_left = w[M + 4];
+    m.steps_packet = w[M + 3];
+    m.flags = w[M + 1];
+    m.aG = w[M + 8];
+    m.aR = w[M + 9];
+    m.aS = w[M + 10];
+    const JobDesc *jd = args.jobs + m.slot;
+    L.jd = jd;
+    L.regions = reinterpret_cast<const RegionConst<T> *>(jd->regions);
+    L.planes = jd->planes;
+    L.adj = reinterpret_cast<const int4 *>(jd->adj);
+    L.px = (T)jd->probe_x;
+    L.py = (T)jd->probe_y;
+    L.pz = (T)jd->probe_z;
+    L.type_bias = jd->type_bias;
+    L.x = get_w<T>(w, 0 * t);
+    L.y = get_w<T>(w, 1 * t);
+    L.z = get_w<T>(w, 2 * t);
+    L.ux = get_w<T>(w, 3 * t);
+    L.uy = get_w<T>(w, 4 * t);
+    L.uz = get_w<T>(w, 5 * t);
+    L.w = get_w<T>(w, 6 * t);
+    L.sleft = get_w<T>(w, 7 * t);
+    L.s_next = get_w<T>(w, 8 * t);
+    L.max_depth = get_w<T>(w, 9 * t);
+    L.lr = get_w<T>(w, 10 * t);
+    L.lr_after = get_w<T>(w, 11 * t);
+    L.loc_fst = get_w<T>(w, 12 * t);
+    L.op = get_w<P>(w, Lay::OP);
+    L.tet = (int32_t)(w[M] & kAdjIndexMask);
+    L.load_region((int)(w[M] >> kAdjIndexBits));
+    L.fst_flag = (m.flags & kFlagFst) ? 1u : 0u;
+    L.stall = m.flags & kStallMask;
+    L.num_back = w[M + 2];
+    L.xG = get_w<unsigned long long>(w, Lay::XG);
+    L.xR = get_w<unsigned long long>(w, Lay::XR);
+    L.xS = get_w<unsigned long long>(w, Lay::XS);
+    L.aG = m.aG;
+    L.aR = m.aR;
+    L.aS = m.aS;
+    L.restores_ = 0;
+    if constexpr (kRecord) {
+        constexpr int R = Lay::REC;
+        L.rhash = get_w<unsigned long long>(w, R);
+        L.rsteps = w[R + 2];
+        L.rhits = w[R + 3];
+        L.rscatters = w[R + 4];
+        L.rrestores = w[R + 5];
+        L.rdetections = w[R + 6];
+        L.rsurvivals = w[R + 7];
+        L.rcontrib = get_w<double>(w, R + 8);
+    }
+}
+
+template <typename T, typename P, bool kRecord>
+__device__ __forceinline__ void pack(const Lane<T, P, kRecord> &L, const PoolMeta &m,
+                                     uint32_t (&w)[PoolLayout<T, P, kRecord>::PADDED]) {
+    using Lay = PoolLayout<T, P, kRecord>;
+    constexpr int t = Lay::t, M = Lay::META;
+#pragma unroll
+    for (int i = Lay::WORDS; i < Lay::PADDED; ++i) w[i] = 0u;
+    put_w(w, 0 * t, L.x);
+    put_w(w, 1 * t, L.y);
+    put_w(w, 2 * t, L.z);
+    put_w(w, 3 * t, L.ux);
+    put_w(w, 4 * t, L.uy);
+    put_w(w, 5 * t, L.uz);
+    put_w(w, 6 * t, L.w);
+    put_w(w, 7 * t, L.sleft);
+    put_w(w, 8 * t, L.s_next);
+    put_w(w, 9 * t, L.max_depth);
+    put_w(w, 10 * t, L.lr);
+    put_w(w, 11 * t, L.lr_after);
+    put_w(w, 12 * t, L.loc_fst);
+    w[M] = (uint32_t)L.tet | ((uint32_t)L.region << kAdjIndexBits);
+    w[M + 1] = (m.flags & kFlagRec) | (L.fst_flag ? kFlagFst : 0u) | (L.stall & kStallMask);
+    w[M + 2] = L.num_back;
+    w[M + 3] = m.steps_packet;
+    w[M + 4] = m.packets_left;
+    w[M + 5] = (uint32_t)m.slot;
+    w[M + 6] = m.lane;
+    w[M + 7] = m.home;
+    w[M + 8] = m.aG;
+    w[M + 9] = m.aR;
+    w[M + 10] = m.aS;
+    w[Lay::OP + 1] = 0u;
+    put_w(w, Lay::OP, L.op);
+    put_w(w, Lay::XG, (unsigned long long)L.xG);
+    put_w(w, Lay::XR, (unsigned long long)L.xR);
+    put_w(w, Lay::XS, (unsigned long long)L.xS);
+    if constexpr (kRecord) {
+        constexpr int R = Lay::REC;
+        put_w(w, R, (unsigned long long)L.rhash);
+        w[R + 2] = L.rsteps;
+        w[R + 3] = L.rhits;
+        w[R + 4] = L.rscatters;
+        w[R + 5] = L.rrestores;
+        w[R + 6] = L.rdetections;
+        w[R + 7] = L.rsurvivals;
+        put_w(w, R + 8, L.rcontrib);
+    }
+}
+
+// Starts unit u (a job's RNG lane): its slot, generators and packet count,
+// and its first packet, with the first step size drawn.  Returns false when
+// the lane has no packets (it is reported finished at once).
+template <typename T, typename P, bool kRecord>
+__device__ __forceinline__ bool start_unit(const LaunchArgs &args, unsigned long long u,
+                                           PacketRecordDev *records, PoolMeta &m,
+                                           Lane<T, P, kRecord> &L) {
+    // the slot holding unit u: the last one whose base is <= u (bases of
+    // empty slots are ~0); read past L1, the host may have filled the slot
+    // after this launch started
+    int lo = 0, hi = args.n_slots - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldcg(args.unit_base + mid) <= u) lo = mid;
+        else hi = mid - 1;
+    }
+    const JobDesc *jd = args.jobs + lo;
+    const uint64_t v = u - __ldcg(args.unit_base + lo);
+    const uint64_t nl = jd->n_lanes;
+    const uint32_t packets = (uint32_t)(jd->n_photons / nl + (v < jd->n_photons % nl ? 1 : 0));
+    if (packets == 0) {
+        unit_finished(args, lo, jd->n_lanes);
+        return false;
+    }
+    m.slot = lo;
+    m.lane = (uint32_t)v;
+    m.packets_left = packets;
+    m.steps_packet = 0;
+    m.flags = (kRecord && records && lo == args.record_slot) ? kFlagRec : 0u;
+    m.aG = jd->rng_a[v];
+    m.aR = jd->rng_aR[v];
+    m.aS = jd->rng_aS[v];
+    L.jd = jd;
+    L.regions = reinterpret_cast<const RegionConst<T> *>(jd->regions);
+    L.planes = jd->planes;
+    L.adj = reinterpret_cast<const int4 *>(jd->adj);
+    L.px = (T)jd->probe_x;
+    L.py = (T)jd->probe_y;
+    L.pz = (T)jd->probe_z;
+    L.type_bias = jd->type_bias;
+    L.region = -1;
+    L.xG = jd->rng_x[v];
+    L.xR = jd->rng_xR[v];
+    L.xS = jd->rng_xS[v];
+    L.aG = m.aG;
+    L.aR = m.aR;
+    L.aS = m.aS;
+    L.restores_ = 0;
+    L.launch();
+    L.draw_step();
+    return true;
+}
+
+// The n-th (from 0) set bit of the 64-bit mask hi:lo.
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t lo, uint32_t hi, int n) {
+    const int c = __popc(lo);
+    return n < c ? (uint32_t)__fns(lo, 0, n + 1) : 32u + (uint32_t)__fns(hi, 0, n - c + 1);
+}
+
+template <typename T, typename P, bool kRecord, int kMinBlocks>
+__global__ void __launch_bounds__(kPoolBlock, kMinBlocks)
+    pooled_kernel(const LaunchArgs args, PacketRecordDev *records, SplitCopy<T, P> *splits) {
+    using Lay = PoolLayout<T, P, kRecord>;
+    extern __shared__ float4 pool_smem[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    const unsigned below = (1u << lane) - 1u;
+    float4 *const pool = pool_smem + (size_t)warp * kPool * Lay::CHUNKS;
+    SplitCopy<T, P> *const wsplit = splits + ((size_t)blockIdx.x * kPoolWarps + warp) * kPool;
+    unsigned int *const err = reinterpret_cast<unsigned int *>(args.ctrl + 2);
+    const int share = args.scatter_share;
+
+    // First units, two per thread, as the per-lane kernel takes them: in a
+    // launch on an idle table thread t takes units start_unit + 2t and
+    // start_unit + 2t + 1; a launch beside a running one claims a run of
+    // 2 x kPoolBlock units per block.
+    __shared__ unsigned long long s_first;
+    __shared__ unsigned s_count;
+    __shared__ unsigned s_busy;  // warps of this block holding photons
+    if (threadIdx.x == 0) {
+        s_busy = kPoolWarps;
+        s_first = 0;
+        s_count = 0;
+        if (args.initial_total == 0) s_count = claim_units(args.ctrl, 2 * kPoolBlock, s_first);
+    }
+    __syncthreads();
+
+    int nA = 0, nB = 0;                    // stack heights (warp-uniform)
+    uint32_t home_lo = 0u, home_hi = 0u;   // free homes (split-copy slots) of the warp
+    {
+        const unsigned long long tid = (unsigned long long)blockIdx.x * kPoolBlock + threadIdx.x;
+#pragma unroll 1
+        for (int r = 0; r < 2; ++r) {
+            unsigned long long u;
+            bool got;
+            if (args.initial_total == 0) {
+                const unsigned idx = (unsigned)(threadIdx.x * 2 + r);
+                u = s_first + idx;
+                got = idx < s_count;
+            } else {
+                u = args.start_unit + 2 * tid + r;
+                got = u < args.initial_total;
+            }
+            PoolMeta m;
+            Lane<T, P, kRecord> L;
+            if (got) got = start_unit<T, P, kRecord>(args, u, records, m, L);
+            const unsigned b = __ballot_sync(full, got);
+            if (got) {
+                m.home = (uint32_t)(r * 32 + lane);
+                uint32_t w[Lay::PADDED];
+                pack(L, m, w);
+                pool_write<Lay>(pool, nA + __popc(b & below), w);
+            }
+            if (r == 0) home_lo = ~b;
+            else home_hi = ~b;
+            nA += __popc(b);
+        }
+        __syncwarp();
+    }
+
+    // Refills and waiting: a warp with free homes takes units from the
+    // counter; after an attempt that found none it retries after kRetryUs,
+    // doubling up to kRetryMaxUs.  A warp without photons waits for jobs
+    // appended while the launch runs; the block leaves once all its warps
+    // have been without photons for linger_us, or when the host drains the
+    // launch.
+    bool waiting = false, last_ok = true;
+    uint32_t idle_since = 0, last_try = 0, gap = kRetryUs;
+
+#pragma unroll 1
+    for (;;) {
+        const int n_free = __popc(home_lo) + __popc(home_hi);
+        uint32_t now = 0;  // the warp's decisions below use lane 0's clock and reads
+        if (n_free > 0) {
+            now = __shfl_sync(full, timer_us(), 0);
+            if (last_ok || now - last_try >= gap) {
+                const int want = n_free < 32 ? n_free : 32;
+                unsigned long long u = 0;
+                bool got = false;
+                if (lane < want) got = take_unit(args.ctrl, u);
+                PoolMeta m;
+                Lane<T, P, kRecord> L;
+                if (got) got = start_unit<T, P, kRecord>(args, u, records, m, L);
+                const unsigned b = __ballot_sync(full, got);
+                if (got) {
+                    const int rank = __popc(b & below);
+                    m.home = nth_set_bit(home_lo, home_hi, rank);
+                    uint32_t w[Lay::PADDED];
+                    pack(L, m, w);
+                    pool_write<Lay>(pool, nA + rank, w);
+                }
+                for (int k = __popc(b); k > 0; --k) {  // the homes taken: the lowest free ones
+                    if (home_lo) home_lo &= home_lo - 1u;
+                    else home_hi &= home_hi - 1u;
+                }
+                nA += __popc(b);
+                last_ok = b != 0u;
+                if (last_ok) {
+                    gap = kRetryUs;
+                } else {
+                    if (gap < kRetryMaxUs) gap <<= 1;
+                    last_try = now;
+                }
+                __syncwarp();
+            }
+        }
+        if (nA + nB == 0) {
+            if (n_free == 0) now = __shfl_sync(full, timer_us(), 0);
+            if (!waiting) {
+                waiting = true;
+                if (lane == 0) atomicSub(&s_busy, 1u);
+                idle_since = now;
+            }
+            __syncwarp();
+            unsigned busy = 0u, drain = 0u;
+            if (lane == 0) {
+                busy = *reinterpret_cast<volatile unsigned *>(&s_busy);
+                drain = __ldcv(args.ctrl + 3) != 0ull ? 1u : 0u;
+            }
+            busy = __shfl_sync(full, busy, 0);
+            drain = __shfl_sync(full, drain, 0);
+            if (busy != 0u) idle_since = now;
+            if (drain || now - idle_since >= args.linger_us) break;
+            __nanosleep(kIdleSleepNs);
+            continue;
+        }
+        if (waiting) {
+            waiting = false;
+            if (lane == 0) atomicAdd(&s_busy, 1u);
+        }
+
+        // ---- one half-step for up to 32 photons of one stack: B once it
+        // holds a warp's worth; with fewer than 32 photons on A, B once it
+        // holds at least share/32 of the warp's photons
+        const bool run_b = nB >= 32 || nA == 0 || (nA < 32 && nB * 32 >= share * (nA + nB));
+        const int mcount = run_b ? min(nB, 32) : min(nA, 32);
+        const bool active = lane < mcount;
+        PoolMeta m;
+        Lane<T, P, kRecord> L;
+        if (active) {
+            uint32_t w[Lay::PADDED];
+            pool_read<Lay>(pool, run_b ? (kPool - nB + lane) : (nA - mcount + lane), w);
+            unpack(w, args, m, L);
+        }
+        __syncwarp();
+        int to = 0;  // 0: leaves the pool, 1: stack A, 2: stack B
+        if (active) {
+            SplitCopy<T, P> &cont = wsplit[m.home];
+            bool end = false, step_done = true;
+            if (run_b) {
+                end = L.phase_b(cont);
+            } else {
+                const int r = L.template phase_a<true>(cont, err);
+                if (r == kPending) step_done = false;
+                else end = r == kEnd;
+            }
+            if (L.restores_) atomicAdd(&L.jd->stats[1], (unsigned long long)L.restores_);
+            if (!step_done) {
+                to = 2;
+            } else {
+                ++m.steps_packet;
+                bool done = end;
+                unsigned reason = 0;
+                if (!done && m.steps_packet >= args.step_cap) {
+                    atomicOr(err, kErrStepCap);
+                    reason = 1;
+                } else if (!done && L.stall >= kStallHits) {
+                    reason = 2;
+                }
+                if (reason) {
+                    atomicAdd(&L.jd->stats[3], 1ull);
+                    done = true;
+                    Incident *inc = args.incident;
+                    if (inc && atomicCAS(&inc->flag, 0u, reason) == 0u) {
+                        inc->slot = (unsigned)m.slot;
+                        inc->tet = L.tet;
+                        inc->packets_left = m.packets_left;
+                        inc->lane = m.lane;
+                        inc->steps = m.steps_packet;
+                        inc->pos[0] = (double)L.x;
+                        inc->pos[1] = (double)L.y;
+                        inc->pos[2] = (double)L.z;
+                        inc->dir[0] = (double)L.ux;
+                        inc->dir[1] = (double)L.uy;
+                        inc->dir[2] = (double)L.uz;
+                        inc->w = (double)L.w;
+                        inc->sleft = (double)L.sleft;
+                    }
+                }
+                if (!done) {
+                    if (L.sleft == (T)0) L.draw_step();
+                    to = 1;
+                } else {
+                    atomicAdd(&L.jd->stats[0], (unsigned long long)m.steps_packet);
+                    atomicAdd(&L.jd->stats[2], 1ull);
+                    if (kRecord && (m.flags & kFlagRec)) {
+                        PacketRecordDev rr;
+                        rr.hash = L.rhash;
+                        rr.x = L.xG;
+                        rr.xR = L.xR;
+                        rr.xS = L.xS;
+                        rr.steps = L.rsteps;
+                        rr.hits = L.rhits;
+                        rr.scatters = L.rscatters;
+                        rr.restores = L.rrestores;
+                        rr.detections = L.rdetections;
+                        rr.survivals = L.rsurvivals;
+                        rr.contribution = L.rcontrib;
+                        rr.optical_path = (double)L.op;
+                        records[m.lane] = rr;
+                        m.flags &= ~kFlagRec;
+                    }
+                    if (--m.packets_left) {
+                        // the unit's next packet, from the same generators
+                        L.launch();
+                        L.draw_step();
+                        m.steps_packet = 0;
+                        to = 1;
+                    } else {
+                        unit_finished(args, m.slot, L.jd->n_lanes);
+                        // the next unit, in the same home
+                        unsigned long long u = 0;
+                        const uint32_t home = m.home;
+                        if (take_unit(args.ctrl, u) &&
+                            start_unit<T, P, kRecord>(args, u, records, m, L)) {
+                            m.home = home;
+                            to = 1;
+                        }
+                    }
+                }
+            }
+        }
+        // ---- push: A grows up from its popped base, B down from its end
+        const int baseA = run_b ? nA : nA - mcount;
+        const int baseB = run_b ? nB - mcount : nB;
+        const unsigned bA = __ballot_sync(full, to == 1);
+        const unsigned bB = __ballot_sync(full, to == 2);
+        if (to) {
+            uint32_t w[Lay::PADDED];
+            pack(L, m, w);
+            pool_write<Lay>(pool, to == 1 ? baseA + __popc(bA & below)
+                                          : kPool - baseB - 1 - __popc(bB & below), w);
+        }
+        // homes of photons that left the pool become free
+        const bool left = active && to == 0;
+        const uint32_t h = left ? m.home : 0u;
+        home_lo |= __reduce_or_sync(full, left && h < 32 ? (1u << h) : 0u);
+        home_hi |= __reduce_or_sync(full, left && h >= 32 ? (1u << (h - 32)) : 0u);
+        nA = baseA + __popc(bA);
+        nB = baseB + __popc(bB);
+        __syncwarp();
+    }
+}
+
 }  // namespace
 
 namespace {
@@ -951,6 +1504,60 @@ const void *photon_kernel_fn(int precision, int min_blocks, bool record) {
         case kFP64: return pick<double, double>(2, record);  // spills at 80 registers
         default: return nullptr;
     }
+}
+
+// Pooled variants: 4, 5 or 6 resident 128-thread blocks per SM (register caps
+// 128, 96 and 80) in the FP32 geometry forms; the FP64 form and the
+// recording variant (16-chunk photon records, 64 KB of shared memory per
+// block) run 2 or 3.
+template <typename T, typename P>
+const void *pick_pooled(int min_blocks, bool record) {
+    if (record) return (const void *)pooled_kernel<T, P, true, 2>;
+    if (sizeof(T) == sizeof(double)) {
+        switch (min_blocks) {
+            case 2: return (const void *)pooled_kernel<T, P, false, 2>;
+            case 3: return (const void *)pooled_kernel<T, P, false, 3>;
+            default: return nullptr;
+        }
+    }
+    switch (min_blocks) {
+        case 4: return (const void *)pooled_kernel<T, P, false, 4>;
+        case 5: return (const void *)pooled_kernel<T, P, false, 5>;
+        case 6: return (const void *)pooled_kernel<T, P, false, 6>;
+        default: return nullptr;
+    }
+}
+
+const void *pooled_kernel_fn(int precision, int min_blocks, bool record) {
+    switch (precision) {
+        case kMixed: return pick_pooled<float, double>(min_blocks, record);
+        case kFP32: return pick_pooled<float, float>(min_blocks, record);
+        case kFP64: return pick_pooled<double, double>(min_blocks, record);
+        default: return nullptr;
+    }
+}
+
+template <typename T, typename P, bool kRecord>
+constexpr size_t pooled_smem() {
+    return (size_t)kPoolWarps * kPool * PoolLayout<T, P, kRecord>::CHUNKS * 16;
+}
+
+size_t pooled_smem_bytes(int precision, bool record) {
+    switch (precision) {
+        case kMixed: return record ? pooled_smem<float, double, true>() : pooled_smem<float, double, false>();
+        case kFP32: return record ? pooled_smem<float, float, true>() : pooled_smem<float, float, false>();
+        default: return record ? pooled_smem<double, double, true>() : pooled_smem<double, double, false>();
+    }
+}
+
+// Opts a pooled variant in to its dynamic shared memory (once per function).
+cudaError_t pooled_prepare(const void *fn, size_t smem) {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, fn);
+    if (e != cudaSuccess) return e;
+    if ((size_t)a.maxDynamicSharedSizeBytes < smem)
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return e;
 }
 
 }  // namespace
@@ -976,6 +1583,44 @@ int photon_kernel_attributes(int precision, int block, int min_blocks, int *regs
     *regs = a.numRegs;
     int nb = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, block, 0);
+    if (e != cudaSuccess) return (int)e;
+    *max_blocks_per_sm = nb;
+    return 0;
+}
+
+size_t pooled_split_bytes(int precision, int grid) {
+    const size_t per = precision == kFP64 ? sizeof(SplitCopy<double, double>)
+                       : precision == kFP32 ? sizeof(SplitCopy<float, float>)
+                                            : sizeof(SplitCopy<float, double>);
+    return (size_t)grid * kPoolWarps * kPool * per;
+}
+
+int launch_pooled_kernel(int precision, int min_blocks, const LaunchArgs &args, int grid,
+                         void *stream, void *records, void *splits) {
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    PacketRecordDev *rec = reinterpret_cast<PacketRecordDev *>(records);
+    const void *fn = pooled_kernel_fn(precision, min_blocks, rec != nullptr);
+    if (!fn || !splits) return (int)cudaErrorInvalidValue;
+    const size_t smem = pooled_smem_bytes(precision, rec != nullptr);
+    cudaError_t e = pooled_prepare(fn, smem);
+    if (e != cudaSuccess) return (int)e;
+    void *params[3] = {const_cast<LaunchArgs *>(&args), &rec, &splits};
+    return (int)cudaLaunchKernel(fn, dim3(grid), dim3(kPoolBlock), params, smem, st);
+}
+
+int pooled_kernel_attributes(int precision, int min_blocks, bool record, int *regs,
+                             int *max_blocks_per_sm) {
+    const void *fn = pooled_kernel_fn(precision, min_blocks, record);
+    if (!fn) return (int)cudaErrorInvalidValue;
+    const size_t smem = pooled_smem_bytes(precision, record);
+    cudaError_t e = pooled_prepare(fn, smem);
+    if (e != cudaSuccess) return (int)e;
+    cudaFuncAttributes a;
+    e = cudaFuncGetAttributes(&a, fn);
+    if (e != cudaSuccess) return (int)e;
+    *regs = a.numRegs;
+    int nb = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kPoolBlock, smem);
     if (e != cudaSuccess) return (int)e;
     *max_blocks_per_sm = nb;
     return 0;

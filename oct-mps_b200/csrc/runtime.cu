@@ -141,6 +141,7 @@ struct Table {
     unsigned error = 0;                    // error word of this table's current batch
     std::vector<octmps_job_id> slot_job;
     std::deque<octmps_job_id> waiting;     // jobs waiting for a free slot
+    void *splits[kMaxLaunches] = {};       // split copies of the pooled kernel, per stream
     std::vector<std::shared_ptr<LaunchRec>> running;  // launches in flight
     std::vector<std::shared_ptr<LaunchRec>> batch;    // launches since the last reset
     Incident last_incident{};              // kept across resets
@@ -329,24 +330,49 @@ octmps_status table_launch(octmps_ctx *ctx, Table &T) {
     if (fresh ? T.next >= T.total
               : (T.total <= T.total_at_launch || (int)T.running.size() >= kMaxLaunches))
         return OCTMPS_OK;
-    // Variant compiled for 2, 3 or 4 resident blocks per SM (register cap
-    // 128, 80 or 64); the FP64 form and the recording variant have only 2.
-    int min_blocks = ctx->cfg.blocks_per_sm >= 2 && ctx->cfg.blocks_per_sm <= 4
+    // The pooled kernel (default): variants for 4, 5 or 6 resident 128-thread
+    // blocks per SM (register caps 128, 96, 80), the FP64 form 2 or 3, the
+    // recording variant 2.  The per-lane kernel: 2, 3 or 4 resident
+    // 256-thread blocks (caps 128, 80, 64); its FP64 form and recording
+    // variant only 2.
+    const bool pooled = ctx->cfg.kernel_form == 0;
+    int min_blocks;
+    if (pooled) {
+        const int want = ctx->cfg.blocks_per_sm;
+        if (T.prec == kFP64) min_blocks = (want == 2 || want == 3) ? want : kDefaultPooledMinBlocksFP64;
+        else min_blocks = (want >= 4 && want <= 6) ? want : kDefaultPooledMinBlocks;
+        if (ctx->record_buf) min_blocks = 2;
+    } else {
+        min_blocks = ctx->cfg.blocks_per_sm >= 2 && ctx->cfg.blocks_per_sm <= 4
                          ? ctx->cfg.blocks_per_sm
                          : kDefaultMinBlocks;
-    if (T.prec == kFP64 || ctx->record_buf) min_blocks = 2;
+        if (T.prec == kFP64 || ctx->record_buf) min_blocks = 2;
+    }
     int regs = 0, per_sm = 0;
-    int st = photon_kernel_attributes(T.prec, 256, min_blocks, &regs, &per_sm);
+    int st = pooled ? pooled_kernel_attributes(T.prec, min_blocks, ctx->record_buf != nullptr, &regs,
+                                               &per_sm)
+                    : photon_kernel_attributes(T.prec, 256, min_blocks, &regs, &per_sm);
     if (st) return cuda_fail(ctx, (cudaError_t)st, "kernel attributes");
     if (per_sm < 1) per_sm = 1;
+    if (pooled && per_sm > 6) per_sm = 6;  // the split-copy buffers hold 6 blocks per SM
+    const int block = pooled ? kPooledBlock : 256;
     const uint64_t grid = (uint64_t)ctx->n_sm * per_sm;
-    const uint64_t threads = grid * 256;
+    // units the launch's threads take first: one per thread (per-lane), two
+    // per thread (pooled)
+    const uint64_t threads = grid * block * (pooled ? kPooledPerThread : 1);
     int si = 0;
     while (si < kMaxLaunches) {
         bool used = false;
         for (auto &r : T.running) used |= r->stream == si;
         if (!used) break;
         ++si;
+    }
+    if (pooled && !T.splits[si]) {
+        // sized for the largest grid of any pooled variant and form (6 blocks
+        // per SM, FP64 split copies); the stream's launches reuse it
+        CK(cudaMallocAsync(&T.splits[si], pooled_split_bytes(kFP64, ctx->n_sm * 6), ctx->stream),
+           "split copies");
+        CK(cudaStreamSynchronize(ctx->stream), "split copies");
     }
     LaunchArgs a;
     a.jobs = T.d_jobs;
@@ -385,7 +411,9 @@ octmps_status table_launch(octmps_ctx *ctx, Table &T) {
     CK(cudaEventCreate(&L->start), "event");
     CK(cudaEventCreate(&L->stop), "event");
     CK(cudaEventRecord(L->start, s), "event");
-    st = launch_photon_kernel(T.prec, min_blocks, a, (int)grid, 256, s, ctx->record_buf);
+    st = pooled ? launch_pooled_kernel(T.prec, min_blocks, a, (int)grid, s, ctx->record_buf,
+                                       T.splits[si])
+                : launch_photon_kernel(T.prec, min_blocks, a, (int)grid, 256, s, ctx->record_buf);
     if (st) return cuda_fail(ctx, (cudaError_t)st, "photon kernel launch");
     CK(cudaEventRecord(L->stop, s), "event");
     T.total_at_launch = T.total;
@@ -674,6 +702,8 @@ octmps_status octmps_ctx_destroy(octmps_ctx *ctx) {
                 t->running.clear();
                 t->batch.clear();
                 cudaFree(t->d_jobs);
+                for (void *p : t->splits)
+                    if (p) cudaFree(p);
                 cudaFreeHost(t->h_state);
                 cudaFreeHost(t->h_ctrl);
                 for (auto s : t->streams) cudaStreamDestroy(s);
@@ -700,8 +730,15 @@ octmps_status octmps_ctx_set_multipliers(octmps_ctx *ctx, const uint32_t *a, uin
 octmps_status octmps_ctx_configure(octmps_ctx *ctx, const octmps_launch_config *cfg) {
     if (!ctx || !cfg) return OCTMPS_ERR_INVALID_ARG;
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
-    if (cfg->block_size != 0 && cfg->block_size != 256)
-        return fail(ctx, OCTMPS_ERR_INVALID_ARG, "block_size must be 256");
+    if (cfg->kernel_form < 0 || cfg->kernel_form > 1)
+        return fail(ctx, OCTMPS_ERR_INVALID_ARG, "kernel_form must be 0 (pooled) or 1 (per-lane)");
+    if (cfg->block_size != 0 && cfg->block_size != (cfg->kernel_form == 1 ? 256 : kPooledBlock))
+        return fail(ctx, OCTMPS_ERR_INVALID_ARG,
+                    "block_size must be 0, 128 (pooled kernel) or 256 (per-lane kernel)");
+    if (cfg->blocks_per_sm != 0 &&
+        (cfg->kernel_form == 1 ? (cfg->blocks_per_sm < 2 || cfg->blocks_per_sm > 4)
+                               : (cfg->blocks_per_sm < 2 || cfg->blocks_per_sm > 6)))
+        return fail(ctx, OCTMPS_ERR_INVALID_ARG, "blocks_per_sm out of range for the kernel form");
     if (cfg->scatter_share < 0 || cfg->scatter_share > 32)
         return fail(ctx, OCTMPS_ERR_INVALID_ARG, "scatter_share must be 0..32");
     if (cfg->linger_us < -1 || cfg->linger_us > 1000000)

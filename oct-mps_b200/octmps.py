@@ -113,7 +113,7 @@ class LaunchConfig(C.Structure):
     _fields_ = [
         ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32), ("default_lanes", C.c_int32),
         ("use_graphs", C.c_int32), ("hbm_budget_bytes", C.c_uint64),
-        ("scatter_share", C.c_int32), ("linger_us", C.c_int32),
+        ("scatter_share", C.c_int32), ("linger_us", C.c_int32), ("kernel_form", C.c_int32),
     ]
 
 
@@ -360,7 +360,7 @@ class Context:
         _check(lib().octmps_ctx_create(device, C.byref(self.h)))
         self._keep = []
         self._cfg = {"blocks_per_sm": 0, "default_lanes": 0, "hbm_budget_bytes": 0,
-                     "scatter_share": 0, "linger_us": 0}
+                     "scatter_share": 0, "linger_us": 0, "kernel_form": 0}
         if multipliers is not None:
             self.set_multipliers(multipliers)
 
@@ -384,46 +384,50 @@ class Context:
 
     def configure(self, **settings):
         """Launch configuration (octmps_launch_config): blocks_per_sm,
-        default_lanes, hbm_budget_bytes, scatter_share, linger_us; settings
-        not given keep their current values (0 = default)."""
+        default_lanes, hbm_budget_bytes, scatter_share, linger_us,
+        kernel_form (0 pooled, 1 per-lane); settings not given keep their
+        current values (0 = default)."""
         unknown = set(settings) - set(self._cfg)
         if unknown:
             raise TypeError(f"unknown launch settings: {sorted(unknown)}")
         cfg = dict(self._cfg, **settings)
         c = LaunchConfig(0, cfg["blocks_per_sm"], cfg["default_lanes"], 0, cfg["hbm_budget_bytes"],
-                         cfg["scatter_share"], cfg["linger_us"])
+                         cfg["scatter_share"], cfg["linger_us"], cfg["kernel_form"])
         _check(lib().octmps_ctx_configure(self.h, C.byref(c)), self.h)
         self._cfg = cfg
 
     def autotune(self, mesh_id, sim, probe_x, root, precision=PREC_MIXED, n_photons=1_000_000,
-                 n_jobs=4, n_lanes=0, blocks=(2, 3), shares=(8, 12, 16, 20, 24), seed=1):
+                 n_jobs=4, n_lanes=0, variants=None, seed=1):
         """Times a sample of the workload (n_jobs jobs of n_photons packets,
         seeds seed..seed+n_jobs-1, in one launch) under each launch variant
-        (resident blocks per SM x scatter share) and keeps the fastest, by
-        propagation steps per second of device time.  The sample should keep
-        the whole GPU busy for most of its launch (lanes well above the
-        resident threads, 75,776 on a 148-SM B200 at 2 blocks/SM), or the
-        launch's tail decides the ranking.
-        Returns (best, [(blocks_per_sm, scatter_share, steps_per_s), ...])."""
+        (kernel form, resident blocks per SM, scatter share) and keeps the
+        fastest, by propagation steps per second of device time.  The sample
+        should keep the whole GPU busy for most of its launch, or the launch's
+        tail decides the ranking.  `variants`: (kernel_form, blocks_per_sm,
+        scatter_share) tuples; by default the pooled kernel at 4-6 blocks/SM
+        and the per-lane kernel at 2-3, each at a few scatter shares.
+        Returns (best, [(kernel_form, blocks_per_sm, scatter_share, steps_per_s), ...])."""
+        if variants is None:
+            variants = [(0, b, sh) for b in (4, 5, 6) for sh in (8, 12, 16)] + \
+                       [(1, b, sh) for b in (2, 3) for sh in (12, 16)]
         nb = sim.num_optical_depth_length_steps
         table = []
-        for b in blocks:
-            for sh in shares:
-                self.configure(blocks_per_sm=b, scatter_share=sh)
-                ids = [self.submit(mesh_id, sim, probe_x, root, n_photons=n_photons,
-                                   seed=seed + k, n_lanes=n_lanes, precision=precision)
-                       for k in range(n_jobs)]
-                self.flush()
-                for j in ids:
-                    self.fetch(j, nb)
-                self.synchronize()
-                sts = [self.stats(j) for j in ids]
-                for j in ids:
-                    self.release(j)
-                ms = {s["launch_id"]: s["device_ms"] for s in sts}
-                table.append((b, sh, sum(s["steps"] for s in sts) / (sum(ms.values()) / 1e3)))
-        best = max(table, key=lambda r: r[2])
-        self.configure(blocks_per_sm=best[0], scatter_share=best[1])
+        for form, b, sh in variants:
+            self.configure(kernel_form=form, blocks_per_sm=b, scatter_share=sh)
+            ids = [self.submit(mesh_id, sim, probe_x, root, n_photons=n_photons,
+                               seed=seed + k, n_lanes=n_lanes, precision=precision)
+                   for k in range(n_jobs)]
+            self.flush()
+            for j in ids:
+                self.fetch(j, nb)
+            self.synchronize()
+            sts = [self.stats(j) for j in ids]
+            for j in ids:
+                self.release(j)
+            ms = {s["launch_id"]: s["device_ms"] for s in sts}
+            table.append((form, b, sh, sum(s["steps"] for s in sts) / (sum(ms.values()) / 1e3)))
+        best = max(table, key=lambda r: r[3])
+        self.configure(kernel_form=best[0], blocks_per_sm=best[1], scatter_share=best[2])
         return best, table
 
     def upload_mesh(self, mesh):

@@ -83,13 +83,19 @@ def assert_records_equal(r_gpu, r_orc):
         assert len(bad) == 0, (f, bad[:5], r_gpu[f][bad[:3]], r_orc[f][bad[:3]])
 
 
+@pytest.mark.parametrize("form", [0, 1])
 @pytest.mark.parametrize("precision", [0, 1, 2])
 @pytest.mark.parametrize("deckname", ["small_deck", "small_matched_deck"])
 def test_first_packets_and_tallies_bit_exact(request, ctx, torch_cuda, octmps, oracle,
-                                             multipliers, precision, deckname):
+                                             multipliers, precision, deckname, form):
+    """Both kernel forms (0 pooled, 1 per-lane) against the oracle."""
     deck = request.getfixturevalue(deckname)
     lanes, n = 3000, 3000  # one packet per lane
-    t_g, st, r_g = run_gpu(ctx, torch_cuda, deck, n, lanes, 985456376, precision)
+    ctx.configure(kernel_form=form)
+    try:
+        t_g, st, r_g = run_gpu(ctx, torch_cuda, deck, n, lanes, 985456376, precision)
+    finally:
+        ctx.configure(kernel_form=0)
     t_o, r_o = run_oracle(oracle, octmps, deck, n, lanes, 985456376, precision, multipliers)
     assert st["packets"] == n
     assert st["steps"] == t_o["steps"] and st["restores"] == t_o["restores"]
@@ -97,12 +103,17 @@ def test_first_packets_and_tallies_bit_exact(request, ctx, torch_cuda, octmps, o
     assert_tallies_equal(t_g, t_o, precision, deck["sim"].num_optical_depth_length_steps)
 
 
+@pytest.mark.parametrize("form", [0, 1])
 @pytest.mark.parametrize("precision", [0, 2])
 def test_many_packets_per_lane_bit_exact(ctx, torch_cuda, octmps, oracle, multipliers, small_deck,
-                                         precision):
+                                         precision, form):
     """Lanes run several packets in a row from the same streams (N % lanes != 0)."""
     lanes, n = 997, 20000
-    t_g, st, r_g = run_gpu(ctx, torch_cuda, small_deck, n, lanes, 5, precision)
+    ctx.configure(kernel_form=form)
+    try:
+        t_g, st, r_g = run_gpu(ctx, torch_cuda, small_deck, n, lanes, 5, precision)
+    finally:
+        ctx.configure(kernel_form=0)
     t_o, r_o = run_oracle(oracle, octmps, small_deck, n, lanes, 5, precision, multipliers)
     assert st["packets"] == n and st["steps"] == t_o["steps"]
     assert_records_equal(r_g, r_o)
@@ -361,20 +372,23 @@ def test_fp32_forms_keep_the_likelihood_finite(ctx, octmps, layers_deck, precisi
 
 
 def test_autotune_picks_a_variant_and_keeps_results(ctx, octmps, small_deck):
-    """The autotuner times each launch variant on a sample and keeps the
-    fastest; the variants change timing only, never the counts."""
+    """The autotuner times each launch variant (kernel form, blocks per SM,
+    scatter share) on a sample and keeps the fastest; the variants change
+    timing only, never the counts."""
     sim = small_deck["sim"]
     nb = sim.num_optical_depth_length_steps
     mid = ctx.upload_mesh(small_deck["mesh"])
+    variants = [(0, 4, 12), (0, 6, 16), (1, 2, 12), (1, 3, 16)]
     best, table = ctx.autotune(mid, sim, 0.0, small_deck["root"], n_photons=100_000,
-                               n_jobs=2, n_lanes=20_000, shares=(12, 16))
-    assert len(table) == 4 and best in table and all(r[2] > 0 for r in table)
+                               n_jobs=2, n_lanes=20_000, variants=variants)
+    assert len(table) == 4 and best in table and all(r[3] > 0 for r in table)
     runs = []
-    for b, sh in ((2, 8), (3, 24)):
-        ctx.configure(blocks_per_sm=b, scatter_share=sh)
+    for form, b, sh in ((0, 5, 8), (0, 6, 24), (1, 2, 8), (1, 3, 24)):
+        ctx.configure(kernel_form=form, blocks_per_sm=b, scatter_share=sh)
         j = ctx.submit(mid, sim, 0.0, small_deck["root"], n_photons=30_000, seed=3, n_lanes=3000)
         runs.append(ctx.fetch(j, nb))
         ctx.release(j)
-    ctx.configure(blocks_per_sm=0, scatter_share=0)
-    assert_tallies_equal(runs[0], runs[1], 0, nb)
+    ctx.configure(kernel_form=0, blocks_per_sm=0, scatter_share=0)
+    for r in runs[1:]:
+        assert_tallies_equal(r, runs[0], 0, nb)
     ctx.release_mesh(mid)
