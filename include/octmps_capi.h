@@ -189,16 +189,17 @@ octmps_status octmps_ctx_set_multipliers(octmps_ctx *ctx, const uint32_t *a, uin
 
 /* Launch configuration (0 = default).  Two forms of the photon kernel run
  * the same per-photon arithmetic:
- *   pooled (kernel_form 0, the default): 128-thread blocks; each warp holds
- *     two photons per lane in shared memory and runs every half of a
- *     propagation step (boundary test, or scattering) on a full warp of
- *     photons at once;
- *   per-lane (kernel_form 1): 256-thread blocks, one photon per thread, a
- *     warp vote choosing which half its lanes run. */
+ *   per-lane (kernel_form 0, the default): 256-thread blocks, one photon per
+ *     thread, a warp vote choosing which half of a propagation step
+ *     (boundary test, or scattering) its lanes run;
+ *   pooled (kernel_form 1): 128-thread blocks; each warp holds two photons
+ *     per lane in shared memory and runs every half-step on a full warp of
+ *     photons at once (fuller warps, but more instructions and fewer
+ *     resident warps: slower on the B-scan workload). */
 typedef struct {
-    int32_t block_size;       /* 0, or the form's block size (128 pooled, 256 per-lane) */
-    int32_t blocks_per_sm;    /* resident blocks per SM: pooled 4, 5 or 6 (0 = 5; the FP64
-                                 form 2 or 3, 0 = 2); per-lane 2, 3 or 4 (0 = 3; FP64 2) */
+    int32_t block_size;       /* 0, or the form's block size (256 per-lane, 128 pooled) */
+    int32_t blocks_per_sm;    /* resident blocks per SM: per-lane 2, 3 or 4 (0 = 3; FP64 2);
+                                 pooled 4, 5 or 6 (0 = 4; the FP64 form 2 or 3, 0 = 2) */
     int32_t default_lanes;    /* RNG lanes per job when job.n_lanes = 0 */
     int32_t use_graphs;       /* reserved, 0 (a batch is one persistent launch, so
                                  there is no launch sequence to replay) */
@@ -212,7 +213,7 @@ typedef struct {
     int32_t linger_us;        /* a kernel thread that finds no work waits this long for
                                  newly submitted jobs before it exits (0 = 2000;
                                  -1 = exit at once; at most 1000000) */
-    int32_t kernel_form;      /* 0 pooled (default), 1 per-lane */
+    int32_t kernel_form;      /* 0 per-lane (default), 1 pooled */
 } octmps_launch_config;
 octmps_status octmps_ctx_configure(octmps_ctx *ctx, const octmps_launch_config *cfg);
 
@@ -307,9 +308,8 @@ octmps_status octmps_write_result(const char *dir, const octmps_sim *sim, double
  *   adj    : int32, 4 per tet (16-byte aligned): -1 for a boundary face, else
  *            neighbour | region_of_neighbour << 24 (meshes below 2^24 tets),
  *            with neighbour < n_tets and 1 <= region < sim->n_regions; the
- *            call does not read this array on the host: the kernel checks
- *            each entry it follows and, on a bad one, ends that packet and
- *            the call returns OCTMPS_ERR_KERNEL
+ *            call checks every entry on the device before any photon runs
+ *            and returns OCTMPS_ERR_INVALID_ARG on a bad one
  *   rng_*  : the lanes' generator states as octmps_rng_init fills them
  *   tally  : OCTMPS_NOALLOC_TALLY_BYTES(nbins) bytes, zeroed by the call:
  *            uint64 totals[4] (filtered, class I, class II, 0) at byte 0, then
@@ -318,7 +318,8 @@ octmps_status octmps_write_result(const char *dir, const octmps_sim *sim, double
  *            16-byte boundary.
  * Errors: OCTMPS_ERR_INVALID_ARG for null pointers, more than
  * OCTMPS_NOALLOC_MAX_REGIONS regions, glass regions (mus = 0), n_lanes 0 or
- * above n_photons, root or tet counts out of range; OCTMPS_ERR_KERNEL if the
+ * above n_photons, root or tet counts out of range, a neighbour entry out of
+ * range; OCTMPS_ERR_KERNEL if the
  * kernel flagged a photon; OCTMPS_ERR_DEVICE on a CUDA error. */
 #define OCTMPS_NOALLOC_MAX_REGIONS 100
 #define OCTMPS_NOALLOC_SCRATCH_BYTES 2640 /* per GPU, held until exit */

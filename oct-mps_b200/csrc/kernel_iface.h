@@ -167,7 +167,7 @@ int photon_kernel_attributes(int precision, int block, int min_blocks, int *regs
 // the photons' split copies, private to the launch.
 constexpr int kPooledBlock = 128;
 constexpr int kPooledPerThread = 2;
-constexpr int kDefaultPooledMinBlocks = 5;
+constexpr int kDefaultPooledMinBlocks = 4;
 constexpr int kDefaultPooledMinBlocksFP64 = 2;
 size_t pooled_split_bytes(int precision, int grid);
 int launch_pooled_kernel(int precision, int min_blocks, const LaunchArgs &args, int grid,

@@ -64,6 +64,23 @@ cudaError_t scratch_address(int device, unsigned char **out) {
     return cudaSuccess;
 }
 
+// The caller's neighbour entries, checked on the device before any photon
+// follows them: each is -1 (ambient) or names a tet below n_tets and a
+// region in [1, n_regions).  A bad entry sets kErrBadNeighbour in the
+// scratch error word.
+__global__ void validate_adj(const int32_t *adj, int64_t n, int32_t n_tets, int32_t n_regions,
+                             unsigned int *err) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t e = adj[i];
+        if (e == -1) continue;
+        const uint32_t idx = (uint32_t)e & kAdjIndexMask;
+        const uint32_t reg = (uint32_t)e >> kAdjIndexBits;
+        if (idx >= (uint32_t)n_tets || reg < 1u || reg >= (uint32_t)n_regions)
+            atomicOr(err, kErrBadNeighbour);
+    }
+}
+
 double div_rd_host(double a, double b) {
     double q = a / b;
     if (!std::isfinite(q) || q == 0.0) return q;
@@ -175,6 +192,18 @@ extern "C" octmps_status octmps_ascan_run_noalloc(const octmps_noalloc_ascan *a,
         return OCTMPS_ERR_INVALID_ARG;
     if (cudaMemsetAsync(a->tally, 0, OCTMPS_NOALLOC_TALLY_BYTES(D.nbins), st) != cudaSuccess)
         return OCTMPS_ERR_DEVICE;
+    unsigned int *err_word = reinterpret_cast<unsigned int *>(scratch + kCtrlOff + 16);
+    {
+        const int64_t n = 4 * (int64_t)a->n_tets;
+        const int64_t blocks = (n + 255) / 256 < (int64_t)sms * 4 ? (n + 255) / 256 : (int64_t)sms * 4;
+        validate_adj<<<(unsigned)blocks, 256, 0, st>>>(a->adj, n, a->n_tets, s.n_regions, err_word);
+        unsigned int bad = 0;
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(&bad, err_word, sizeof bad, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return OCTMPS_ERR_DEVICE;
+        if (bad) return OCTMPS_ERR_INVALID_ARG;  // a neighbour entry names no tet or region
+    }
     LaunchArgs L;
     L.jobs = reinterpret_cast<const JobDesc *>(scratch + kJobOff);
     L.unit_base = reinterpret_cast<const uint64_t *>(scratch + kUnitOff);

@@ -443,10 +443,10 @@ struct Lane {
     // Returns kDone, kEnd (the packet ended) or kPending (no face reached:
     // the step continues in phase_b).
     // ComputeStepSize's draw for a step that starts with sleft == 0,
-    // src/octmps_kernel.cuh:505-515.  The pooled kernel draws it at the end
-    // of the previous step (after its roulette and stop checks) or at the
-    // launch: the general stream's draws keep their order, and the first half
-    // of a step no longer diverges on the logarithm.
+    // src/octmps_kernel.cuh:505-515.  The kernels draw it at the end of the
+    // previous step (after its roulette and stop checks) or at the launch:
+    // the general stream's draws keep their order, and the first half of a
+    // step no longer diverges on the logarithm.
     __device__ __forceinline__ void draw_step() {
         const T r = (T)1 - rand_co_G();
         s_next = -log_method(r) * rg.rmuas;
@@ -536,14 +536,6 @@ struct Lane {
             const T ca1 = -min_cos;
             const int32_t entry = face == 0 ? nb.x : face == 1 ? nb.y : face == 2 ? nb.z : nb.w;
             const int next_region = entry < 0 ? 0 : (int)((uint32_t)entry >> kAdjIndexBits);
-            // A neighbour entry must name a tet of the mesh and a region of
-            // the job's table: the job API checks the mesh at upload, the
-            // allocation-free entry point takes the caller's array unchecked.
-            if (entry >= 0 && (next_region >= jd->n_regions ||
-                               (int32_t)((uint32_t)entry & kAdjIndexMask) >= jd->n_tets)) {
-                atomicOr(err, kErrBadNeighbour);
-                return kEnd;
-            }
             const T nt = entry < 0 ? (T)jd->n_ambient
                                    : __ldg(reinterpret_cast<const T *>(regions + next_region));
             T r;
@@ -844,6 +836,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
                     unit_finished(args, lg.slot, jd->n_lanes);
                 } else {
                     L.launch();
+                    L.draw_step();
                     steps_packet = 0;
                     pending = false;
                     recording = kRecord && records && lo == args.record_slot;
@@ -867,7 +860,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
             end = L.phase_b(cont);
         } else {
             if (pending) continue;
-            const int r = L.phase_a(cont, err);
+            const int r = L.template phase_a<true>(cont, err);
             if (r == kPending) {
                 pending = true;
                 continue;
@@ -910,6 +903,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
                 inc->sleft = (double)L.sleft;
             }
         }
+        if (!done && L.sleft == (T)0) L.draw_step();  // the next step's size, drawn ahead
         if (done) {
             // per-packet statistics: steps, split copies resumed, packets
             atomicAdd(&L.jd->stats[0], (unsigned long long)steps_packet);
@@ -936,6 +930,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
             --packets_left;
             if (packets_left) {
                 L.launch();
+                L.draw_step();
                 steps_packet = 0;
             } else {
                 unit_finished(args, lg.slot, L.jd->n_lanes);
@@ -962,6 +957,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
 // starts with sleft == 0 is drawn at the end of the previous step (after its
 // roulette and stop checks) or at the launch, which keeps the general
 // stream's draws in order and takes the logarithm out of the boundary half.
+//
+// Measured on the B-scan workload (8 A-scans x 2e5 packets, B200): the
+// pooled form raises active threads per warp instruction from 15.7 to 23.5,
+// but spends 44 % more thread instructions (moving photon state and reloading
+// job constants every half-step) and, at 128 registers, keeps 16 warps per SM
+// resident against the per-lane kernel's 24 (issue active 48 % vs 60 %):
+// 28.9 G against 37.7 G propagation steps/s.  It is kept as a launch variant
+// (octmps_launch_config.kernel_form = 1) that the autotuner times.
 //
 // A photon's state is 16-byte chunks (8 for the mixed and FP32 forms, 16 for
 // FP64 and the recording variant); chunk k of the photon at position q sits

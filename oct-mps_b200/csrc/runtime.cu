@@ -330,12 +330,11 @@ octmps_status table_launch(octmps_ctx *ctx, Table &T) {
     if (fresh ? T.next >= T.total
               : (T.total <= T.total_at_launch || (int)T.running.size() >= kMaxLaunches))
         return OCTMPS_OK;
-    // The pooled kernel (default): variants for 4, 5 or 6 resident 128-thread
-    // blocks per SM (register caps 128, 96, 80), the FP64 form 2 or 3, the
-    // recording variant 2.  The per-lane kernel: 2, 3 or 4 resident
-    // 256-thread blocks (caps 128, 80, 64); its FP64 form and recording
-    // variant only 2.
-    const bool pooled = ctx->cfg.kernel_form == 0;
+    // The per-lane kernel (default): 2, 3 or 4 resident 256-thread blocks per
+    // SM (register caps 128, 80, 64); its FP64 form and recording variant
+    // only 2.  The pooled kernel: 4, 5 or 6 resident 128-thread blocks
+    // (caps 128, 96, 80), the FP64 form 2 or 3, the recording variant 2.
+    const bool pooled = ctx->cfg.kernel_form == 1;
     int min_blocks;
     if (pooled) {
         const int want = ctx->cfg.blocks_per_sm;
@@ -731,12 +730,12 @@ octmps_status octmps_ctx_configure(octmps_ctx *ctx, const octmps_launch_config *
     if (!ctx || !cfg) return OCTMPS_ERR_INVALID_ARG;
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     if (cfg->kernel_form < 0 || cfg->kernel_form > 1)
-        return fail(ctx, OCTMPS_ERR_INVALID_ARG, "kernel_form must be 0 (pooled) or 1 (per-lane)");
-    if (cfg->block_size != 0 && cfg->block_size != (cfg->kernel_form == 1 ? 256 : kPooledBlock))
+        return fail(ctx, OCTMPS_ERR_INVALID_ARG, "kernel_form must be 0 (per-lane) or 1 (pooled)");
+    if (cfg->block_size != 0 && cfg->block_size != (cfg->kernel_form == 0 ? 256 : kPooledBlock))
         return fail(ctx, OCTMPS_ERR_INVALID_ARG,
-                    "block_size must be 0, 128 (pooled kernel) or 256 (per-lane kernel)");
+                    "block_size must be 0, 256 (per-lane kernel) or 128 (pooled kernel)");
     if (cfg->blocks_per_sm != 0 &&
-        (cfg->kernel_form == 1 ? (cfg->blocks_per_sm < 2 || cfg->blocks_per_sm > 4)
+        (cfg->kernel_form == 0 ? (cfg->blocks_per_sm < 2 || cfg->blocks_per_sm > 4)
                                : (cfg->blocks_per_sm < 2 || cfg->blocks_per_sm > 6)))
         return fail(ctx, OCTMPS_ERR_INVALID_ARG, "blocks_per_sm out of range for the kernel form");
     if (cfg->scatter_share < 0 || cfg->scatter_share > 32)

@@ -385,7 +385,7 @@ class Context:
     def configure(self, **settings):
         """Launch configuration (octmps_launch_config): blocks_per_sm,
         default_lanes, hbm_budget_bytes, scatter_share, linger_us,
-        kernel_form (0 pooled, 1 per-lane); settings not given keep their
+        kernel_form (0 per-lane, 1 pooled); settings not given keep their
         current values (0 = default)."""
         unknown = set(settings) - set(self._cfg)
         if unknown:
@@ -404,12 +404,12 @@ class Context:
         fastest, by propagation steps per second of device time.  The sample
         should keep the whole GPU busy for most of its launch, or the launch's
         tail decides the ranking.  `variants`: (kernel_form, blocks_per_sm,
-        scatter_share) tuples; by default the pooled kernel at 4-6 blocks/SM
-        and the per-lane kernel at 2-3, each at a few scatter shares.
+        scatter_share) tuples; by default the per-lane kernel at 2-3 blocks/SM
+        and the pooled kernel at 4-5, each at a few scatter shares.
         Returns (best, [(kernel_form, blocks_per_sm, scatter_share, steps_per_s), ...])."""
         if variants is None:
-            variants = [(0, b, sh) for b in (4, 5, 6) for sh in (8, 12, 16)] + \
-                       [(1, b, sh) for b in (2, 3) for sh in (12, 16)]
+            variants = [(0, b, sh) for b in (2, 3) for sh in (8, 10, 12, 14, 16)] + \
+                       [(1, b, sh) for b in (4, 5) for sh in (12,)]
         nb = sim.num_optical_depth_length_steps
         table = []
         for form, b, sh in variants:

@@ -126,11 +126,11 @@ def test_noalloc_entry_point_matches_job_api(octmps, small_deck):
 
 
 def test_noalloc_bad_neighbour_entries_are_reported(octmps, small_deck):
-    """The caller's neighbour array is not read on the host; the kernel checks
-    each entry it follows.  Both cases keep every access in bounds even
-    without the check (a region below the fixed table's 100 entries; arrays
-    allocated for the whole mesh while n_tets claims half of it), so the test
-    shows the report, not a fault."""
+    """The caller's neighbour array is checked on the device before any
+    photon follows it.  Both cases keep every access in bounds even without
+    the check (a region below the fixed table's 100 entries; arrays allocated
+    for the whole mesh while n_tets claims half of it), so the test shows the
+    report, not a fault."""
     torch = pytest.importorskip("torch")
     assert torch.cuda.is_available()
     sim, mesh, root = small_deck["sim"], small_deck["mesh"], small_deck["root"]
@@ -140,10 +140,10 @@ def test_noalloc_bad_neighbour_entries_are_reported(octmps, small_deck):
     a, dev, f, stream = noalloc_call(
         octmps, torch, sim, mesh, root, lanes, n, seed, mult,
         adj_override=lambda adj: np.where(adj < 0, -1, (adj & 0xFFFFFF) | (bad_region << 24)))
-    assert f(C.byref(a), C.c_void_p(stream)) == 9  # OCTMPS_ERR_KERNEL
+    assert f(C.byref(a), C.c_void_p(stream)) == 1  # OCTMPS_ERR_INVALID_ARG
     a, dev, f, stream = noalloc_call(octmps, torch, sim, mesh, root, lanes, n, seed, mult)
     assert root < mesh.n_tets // 2
     a.n_tets = mesh.n_tets // 2  # neighbours in the second half are out of range
-    assert f(C.byref(a), C.c_void_p(stream)) == 9
+    assert f(C.byref(a), C.c_void_p(stream)) == 1
     a.n_tets = mesh.n_tets  # the next call starts clean
     assert f(C.byref(a), C.c_void_p(stream)) == 0
