@@ -21,6 +21,8 @@ CENSUS_FIELDS = ("add", "mul", "div", "sqrt", "fma", "trans")
 REF_SO = os.path.join(HERE, "_ref", "libocref.so")
 # the same sources built -O3 -march=x86-64-v4 with contraction: the timed CPU baseline
 REF_FAST_SO = os.path.join(HERE, "_ref", "libocref_fast.so")
+# the same sources with log and sincos routed to the oracle's series
+REF_METHOD_SO = os.path.join(HERE, "_ref", "libocref_method.so")
 MAX_REGIONS = 100
 
 P = C.POINTER

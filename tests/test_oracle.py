@@ -222,3 +222,56 @@ def test_operation_census_runs_the_oracle_and_matches_the_frozen_f_step(octmps, 
             np.testing.assert_array_equal(t_c[k], t_o[k], err_msg=k)
         assert abs(counts["flops_per_step"] / bench.F_STEP[prec] - 1) < 0.02, counts
 
+
+
+def method_reference():
+    try:
+        return oracle_py.Reference(oracle_py.REF_METHOD_SO)
+    except ImportError as e:
+        pytest.skip(f"reference host build unavailable: {e}")
+
+
+def packets_identical(rec_r, rec_o):
+    return ((rec_r["hash"] == rec_o["hash"]) & (rec_r["x"] == rec_o["x"]) &
+            (rec_r["xR"] == rec_o["xR"]) & (rec_r["xS"] == rec_o["xS"]) &
+            (rec_r["steps"] == rec_o["steps"]) & (rec_r["detections"] == rec_o["detections"]) &
+            (rec_r["restores"] == rec_o["restores"]) &
+            (rec_r["optical_path"] == rec_o["optical_path"]))
+
+
+@pytest.mark.parametrize("deck", ["Sphere", "bscan"])
+def test_fp64_oracle_is_the_reference_method_bit_for_bit(oracle, octmps, meshgen, workdir, deck):
+    """With the reference's log and sincos routed to the oracle's series
+    (oracle/_ref/libocref_method.so; acos and every other operation the
+    reference's own), the FP64 restatement reproduces the reference routine
+    packet for packet: event sequence, generator states, steps, detections,
+    restores and optical path of every first packet identical, contributions
+    equal to summation order.  So the differences against the glibc build
+    (test_fp64_first_packets_match_reference) are transcendental last bits
+    only.  Decks: the reference's Sphere (2000 lanes) and the B-scan workload
+    at three positions (1000 lanes each, ~12,000-15,000 steps per packet)."""
+    R = method_reference()
+    if deck == "Sphere":
+        opt, mesh_path, mci = ref_deck_paths("Sphere")
+        cases = [(None, 985456376, 2000)]
+    else:
+        p = meshgen.config_bscan(os.path.join(workdir, "bscan_method"))
+        opt, mesh_path, mci = p["opt"], p["mesh"], p["mci"]
+        cases = [(k, k + 1, 1000) for k in (0, 128, 255)]
+    sim = octmps.read_deck(opt, mci)
+    mesh = octmps.build_mesh(mesh_path)
+    rs = R.parse(opt, mci)
+    xs = octmps.probe_positions(sim)
+    for k, seed, n in cases:
+        x = sim.start_x if k is None else xs[k]
+        root = mesh.find_root(x)
+        rng = octmps.rng_init(octmps.safeprimes(3 + 3 * n), n, seed)
+        rec_r = R.trace(rs, mesh, root, (x, 0, 0), {a: b.copy() for a, b in rng.items()}, n)
+        _, rec_o = oracle.run(oracle_py.params_from_sim(sim), mesh, (x, 0, 0), root, n, n,
+                              {a: b.copy() for a, b in rng.items()}, 2, record=True)
+        same = packets_identical(rec_r, rec_o)
+        assert same.all(), (deck, k, np.where(~same)[0][:5])
+        c_r, c_o = rec_r["contribution"], rec_o["contribution"]
+        nz = c_r != 0
+        assert np.all(np.abs(c_o[nz] - c_r[nz]) <= 1e-14 * np.abs(c_r[nz]))
+        assert np.array_equal(c_o[~nz], c_r[~nz])
