@@ -239,6 +239,8 @@ def run_ours(args, rank, world, local_rank, dist):
         torch.cuda.synchronize()
 
     mid = ctx.upload_mesh(mesh)
+    if args.kernel_form is not None or args.blocks_per_sm:
+        ctx.configure(kernel_form=args.kernel_form or 0, blocks_per_sm=args.blocks_per_sm)
     tuned = None
     if args.autotune:
         tuned = autotune(ctx, mid, sim, xs, roots, args, lanes)
@@ -384,6 +386,39 @@ def run_ours(args, rank, world, local_rank, dist):
     }
 
 
+def run_serving(args):
+    """--serve: the served request stream (four resident meshes of 50k, 381k,
+    994k and 2.0M tets; Poisson arrivals of A-scan requests of 1e5-1e7
+    packets and 32-128-A-scan B-scan requests of 1e5 packets each at 3:1),
+    capacity measured on a Poisson stream, then offered loads of 0.5, 0.9 and
+    1.2 x capacity with --serve-requests requests each."""
+    import serve
+    work = tempfile.mkdtemp(prefix="octmps_serve_")
+    meshes = serve.build_meshes("full", work)
+    import octmps
+    max_lanes = 1 << 18
+    ctx = octmps.Context(0, octmps.safeprimes(3 + 3 * max_lanes))
+    for m in meshes.values():
+        m["id"] = ctx.upload_mesh(m["mesh"])
+    sampler = ClockSampler(0)
+    sampler.start()
+    res = serve.serve_levels(ctx, meshes, [0.5, 0.9, 1.2], args.serve_requests, 1.0, max_lanes,
+                             log=lambda d: print(json.dumps(d), file=sys.stderr, flush=True))
+    clocks = sampler.stop()
+    ctx.close()
+    top = res["levels"][-1]
+    return {
+        "metric": "served stream: packets/s and p50/p99 latency per request type",
+        "value": top["throughput_packets_per_s"], "unit": "packets/s", "n_gpus": 1,
+        "impl": "ours", "higher_is_better": True, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": "served stream, meshes " + ", ".join(
+            f"{k} {m['n_tets']} tets" for k, m in meshes.items()) +
+            f"; {args.serve_requests} requests per load level", "loads": [0.5, 0.9, 1.2]},
+        "serving": res, "clocks": clocks,
+        "note": "value = throughput at offered load 1.2 x capacity",
+    }
+
+
 def reference_inputs(args):
     """The workload as the reference itself reads it, without the product
     library: the deck files (meshgen writes input files only), parsed by the
@@ -512,11 +547,22 @@ def main():
                     help="A-scans of the ours-arm cpu_baseline sample")
     ap.add_argument("--cpu-packets", type=int, default=4800,
                     help="packets per A-scan of the ours-arm cpu_baseline sample")
+    ap.add_argument("--serve", action="store_true",
+                    help="run the served-stream study instead of the B-scan bench")
+    ap.add_argument("--serve-requests", type=int, default=200,
+                    help="requests per offered-load level of --serve")
+    ap.add_argument("--kernel-form", type=int, default=None,
+                    help="0 per-lane, 1 pooled (default: the library's, or --autotune's)")
+    ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--ref-packets", type=int, default=1200,
                     help="packets per A-scan of each --impl reference step")
     args = ap.parse_args()
     rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
     local_rank = env_int("LOCAL_RANK", 0)
+
+    if args.serve:
+        print(json.dumps(run_serving(args)), flush=True)
+        return
 
     if args.impl == "reference":
         out = run_reference(args, rank, world)

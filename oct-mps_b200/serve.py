@@ -11,6 +11,7 @@ records each request's latency (arrival to last A-scan fetched).  Throughput
 (packets/s) and p50/p99 latency per request type are reported.
 
     python serve.py [--loads 0.5,0.9,1.2] [--requests 24] [--scale small|full]
+    python bench.py --serve          (the full study, recorded as a bench line)
 """
 import argparse
 import json
@@ -244,6 +245,57 @@ def run_stream(server, reqs, speed=1.0):
     return time.perf_counter() - t0
 
 
+def serve_levels(ctx, meshes, loads, n_requests, photon_scale=1.0, max_lanes=1 << 18,
+                 n_calibration=None, log=None):
+    """The served-stream study: capacity, then each offered load.
+
+    Capacity is measured on a Poisson stream, not with every request queued
+    at once: a first estimate c0 comes from a queued batch of
+    n_calibration requests; a Poisson stream offered at 1.5 x c0 then runs
+    n_requests requests, and its sustained throughput (packets completed /
+    time from the first arrival to the last completion) is the capacity.
+    Each load level then offers load x capacity in Poisson arrivals
+    (seeded streams) of n_requests requests; throughput, p50/p99 latency per
+    request type and how many requests overlapped another on the GPU are
+    reported."""
+    n_cal = n_calibration or max(8, n_requests // 8)
+    cal = make_stream(meshes, n_cal, 1e9, np.random.default_rng(55), photon_scale)
+    srv = Server(ctx, meshes, max_lanes=max_lanes)
+    wall = run_stream(srv, cal)
+    c0 = srv.packets_done / wall
+    per_req0 = srv.packets_done / len(cal)
+    srv.close()
+    sat = make_stream(meshes, n_requests, 1.5 * c0 / per_req0, np.random.default_rng(56),
+                      photon_scale)
+    srv = Server(ctx, meshes, max_lanes=max_lanes)
+    wall = run_stream(srv, sat)
+    srv.close()
+    capacity = srv.packets_done / wall
+    work_per_req = srv.packets_done / len(sat)
+    out = {"queued_estimate_packets_per_s": c0, "capacity_packets_per_s": capacity,
+           "capacity_stream": {"requests": len(sat), "offered_packets_per_s": 1.5 * c0,
+                               "wall_s": wall, "latency": latency_stats([r for _, r in sat])},
+           "mean_packets_per_request": work_per_req, "levels": [], "errors": srv.errors[:3]}
+    if log:
+        log(out)
+    rng = np.random.default_rng(5)
+    for load in loads:
+        rate = load * capacity / work_per_req
+        reqs = make_stream(meshes, n_requests, rate, rng, photon_scale)
+        srv = Server(ctx, meshes, max_lanes=max_lanes)
+        wall = run_stream(srv, reqs)
+        srv.close()
+        done = [r for _, r in reqs]
+        lvl = {"offered_load": load, "arrival_rate_hz": rate, "requests": len(done),
+               "wall_s": wall, "throughput_packets_per_s": srv.packets_done / wall,
+               "offered_packets_per_s": rate * work_per_req, "latency": latency_stats(done),
+               "errors": srv.errors[:3], "requests_overlapping_another": overlapping(done)}
+        out["levels"].append(lvl)
+        if log:
+            log(lvl)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--loads", default="0.5,0.9,1.2")
@@ -260,29 +312,9 @@ def main():
     with octmps.Context(args.device, mult) as ctx:
         for m in meshes.values():
             m["id"] = ctx.upload_mesh(m["mesh"])
-        # capacity: packets/s with every request queued at once
-        cal = make_stream(meshes, args.requests, 1e9, np.random.default_rng(55), args.photon_scale)
-        srv = Server(ctx, meshes, max_lanes=max_lanes)
-        wall = run_stream(srv, cal)
-        cap_pkts = srv.packets_done / wall
-        work_per_req = srv.packets_done / len(cal)
-        srv.close()
-        print(json.dumps({"capacity_packets_per_s": cap_pkts, "requests": len(cal),
-                          "mean_packets_per_request": work_per_req, "errors": srv.errors[:3],
-                          "meshes": {k: m["n_tets"] for k, m in meshes.items()}}), flush=True)
-        for load in [float(v) for v in args.loads.split(",")]:
-            rate = load * cap_pkts / work_per_req
-            reqs = make_stream(meshes, args.requests, rate, rng, args.photon_scale)
-            srv = Server(ctx, meshes, max_lanes=max_lanes)
-            wall = run_stream(srv, reqs)
-            srv.close()
-            done = [r for _, r in reqs]
-            print(json.dumps({
-                "offered_load": load, "arrival_rate_hz": rate, "wall_s": wall,
-                "throughput_packets_per_s": srv.packets_done / wall,
-                "latency": latency_stats(done), "errors": srv.errors[:3],
-                "requests_overlapping_another": overlapping(done)}), flush=True)
-
+        serve_levels(ctx, meshes, [float(v) for v in args.loads.split(",")], args.requests,
+                     args.photon_scale, max_lanes,
+                     log=lambda d: print(json.dumps(d), flush=True))
 
 if __name__ == "__main__":
     main()
