@@ -311,6 +311,18 @@ def run_ours(args, rank, world, local_rank, dist):
                 "frac_of_fp64_peak": s64 / (d64 / 1e3) * F_STEP_FP64 /
                 (fp_peak_tflops(clocks, 64) * 1e12)}
 
+    # The 64 batched uneven jobs (each its own mesh of 46k-744k tets, 1.3e4-
+    # 9.6e6 packets): one job table against one launch per job.
+    uneven = None
+    if args.uneven_jobs > 0 and world == 1:
+        import batch_uneven
+        t0 = time.perf_counter()
+        ujobs = batch_uneven.build_jobs(args.uneven_jobs, os.path.join(work, "uneven"))
+        uneven = batch_uneven.run(ctx, ujobs)
+        uneven["host_mesh_build_s"] = time.perf_counter() - t0 - uneven["batched"]["wall_s"] - \
+            uneven["plain"]["wall_s"]
+        del ujobs
+
     t_dev = torch.tensor([dev_ms, e2e_ms / e2e_steps], dtype=torch.float64, device="cuda")
     if dist is not None:
         dist.all_reduce(t_dev, op=dist.ReduceOp.MAX)
@@ -380,6 +392,7 @@ def run_ours(args, rank, world, local_rank, dist):
         },
         "clocks": clocks,
         "plain_single_job": plain,
+        "uneven_jobs": uneven,
         "fp64": fp64,
         "autotune": tuned,
         "first_timed_position": first_timed * batch % len(xs),
@@ -537,10 +550,14 @@ def main():
     ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--lanes", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--autotune", action="store_true",
-                    help="choose the launch variant on a sample before timing")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="skip choosing the launch variant on a sample before timing")
     ap.add_argument("--plain-ascans", type=int, default=4,
                     help="A-scans run one per launch for the batched-over-plain ratio")
+    ap.add_argument("--ref-gpu-ascans", type=int, default=2,
+                    help="A-scans the reference's own CUDA build runs (0: skip)")
+    ap.add_argument("--uneven-jobs", type=int, default=64,
+                    help="batched uneven jobs, one table vs one launch per job (0: skip)")
     ap.add_argument("--fp64-ascans", type=int, default=8,
                     help="A-scans of the first timed step rerun in the FP64 form")
     ap.add_argument("--cpu-ascans", type=int, default=8,
@@ -580,6 +597,20 @@ def main():
                               device_id=torch.device("cuda", local_rank))
         dist = td
     out = run_ours(args, rank, world, local_rank, dist)
+    if rank == 0 and world == 1 and args.ref_gpu_ascans > 0:
+        # the reference's own CUDA program on the same GPU, on the first
+        # A-scans of the first timed step (baseline/run_ref_gpu.py)
+        sys.path.insert(0, os.path.join(ROOT, "baseline"))
+        try:
+            import run_ref_gpu
+            out["reference_gpu"] = run_ref_gpu.run(first=out["first_timed_position"],
+                                                   ascans=args.ref_gpu_ascans,
+                                                   photons=args.photons, timeout_s=600)
+        except Exception as e:  # the baseline never hides the GPU result
+            out["reference_gpu"] = {"unavailable": f"{type(e).__name__}: {e}"}
+        rg = out["reference_gpu"]
+        if rg.get("value"):
+            rg["ours_over_reference"] = out["value"] / rg["value"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # the reference's routine on the host cores, on the A-scans of the
         # first timed step (a bounded sample, about 10 s)

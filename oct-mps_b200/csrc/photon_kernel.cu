@@ -539,13 +539,19 @@ struct Lane {
             const T nt = entry < 0 ? (T)jd->n_ambient
                                    : __ldg(reinterpret_cast<const T *>(regions + next_region));
             T r;
-            T sa1 = sqrtT(DevNum<T>::mad(-ca1, ca1, (T)1));
-            if (ca1 > DevNum<T>::coszero) sa1 = 0;
+            const T sa1_sq = DevNum<T>::mad(-ca1, ca1, (T)1);
             if (kFused<T> && rg.n == nt) {
                 // FP32 forms, matched refractive indices: R is exactly 0
                 // except for the grazing-incidence rule (sa2 = sa1 here).
-                r = (ca1 < DevNum<T>::cos90 || sa1 == (T)1) ? (T)1 : (T)0;
+                // sa1 = sqrt(1 - ca1^2) is 1 exactly when its argument is 1
+                // (the correctly rounded root of the largest float below 1
+                // is below 1), and 0 when ca1 > COSZERO: no root needed.
+                r = (ca1 < DevNum<T>::cos90 || (sa1_sq == (T)1 && !(ca1 > DevNum<T>::coszero)))
+                        ? (T)1
+                        : (T)0;
             } else {
+                T sa1 = sqrtT(sa1_sq);
+                if (ca1 > DevNum<T>::coszero) sa1 = 0;
                 const T ni_nt = DevNum<T>::div(rg.n, nt);
                 const T sa2 = fminT(ni_nt * sa1, (T)1);
                 const T ca2 = sqrtT(DevNum<T>::mad(-sa2, sa2, (T)1));

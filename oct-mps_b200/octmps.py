@@ -408,8 +408,8 @@ class Context:
         and the pooled kernel at 4-5, each at a few scatter shares.
         Returns (best, [(kernel_form, blocks_per_sm, scatter_share, steps_per_s), ...])."""
         if variants is None:
-            variants = [(0, b, sh) for b in (2, 3) for sh in (8, 10, 12, 14, 16)] + \
-                       [(1, b, sh) for b in (4, 5) for sh in (12,)]
+            variants = [(0, b, sh) for b in (2, 3) for sh in (10, 12, 14)] + \
+                       [(1, b, 12) for b in (4, 5)]
         nb = sim.num_optical_depth_length_steps
         table = []
         for form, b, sh in variants:
