@@ -10,7 +10,7 @@ under total internal reflection) and the four-layer precision slab
 * Statistical: per-bin Class I/II means of the mixed form against the FP64
   form (both on the GPU, independent seeds) and against the reference's own
   routine (src/octmps_kernel.cuh:1329-1402, committed fixtures from
-  tests/golden/make_bscan_golden.py), with the per-bin standard error of
+  tests/golden/make_parity_golden.py), with the per-bin standard error of
   src/octmps_io.cpp:310-318 and a Bonferroni bound over the bins compared.
 """
 import math
