@@ -198,3 +198,30 @@ def test_cli_usage_without_arguments():
     r = subprocess.run([exe], capture_output=True, text=True)
     assert r.returncode == 1
     assert "Usage:" in r.stdout and "-S<seed>" in r.stdout
+
+
+def test_mesh_builder_matches_reference_on_the_bscan_mesh(octmps, meshgen, workdir):
+    """The product's O(T) builder against the reference's own MeshGraph +
+    SerializeGraph + FindRootofGraph on the benchmark's 380,928-tet B-scan
+    mesh (their output cached by oracle/ref_mesh_cache.py, about two hours of
+    the reference's O(T^2) face matching): every tet's region, faces, signs
+    and neighbours, every distinct face plane and the root of every one of
+    the 256 probe positions identical."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_mesh_cache
+    p = meshgen.config_bscan(os.path.join(workdir, "bscan_refmesh"))
+    try:
+        c = ref_mesh_cache.load(p["mesh"])
+    except FileNotFoundError as e:
+        pytest.skip(str(e))
+    m = octmps.build_mesh(p["mesh"])
+    np.testing.assert_array_equal(m.region, c["tet"][:, 1])
+    np.testing.assert_array_equal(m.faces, c["tet"][:, 2:6])
+    np.testing.assert_array_equal(m.signs, c["tet"][:, 6:10])
+    np.testing.assert_array_equal(m.adj, c["tet"][:, 10:14])
+    assert m.n_distinct == len(c["planes"])
+    np.testing.assert_array_equal(m.planes[: len(c["planes"])], c["planes"])
+    xs = octmps.probe_positions(octmps.read_deck(p["opt"], p["mci"]))
+    np.testing.assert_array_equal(np.asarray(xs), c["xs"])
+    assert [m.find_root(x) for x in xs] == [int(r) for r in c["roots"]]
