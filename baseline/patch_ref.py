@@ -8,6 +8,14 @@ committed) and applies the measurement patches of its CUDA build:
   * a cap of MAX_LAUNCHES relaunches per A-scan, so that a packet that never
     ends (the reference has no step limit) cannot keep the loop going.
 
+  * the reference selects its launch settings for "compute capability 3.5"
+    (600 threads per block) by defining the compiler's own __CUDA_ARCH__
+    macro to 350 in src/octmps_kernel.h:61 and testing it in :67-97 and
+    src/main.cu:978; defined in the host pass that macro marks host code
+    as device code to CUDA's headers and to the launch stubs nvcc appends, and
+    the build crashes at run time.  The same selection is made through a macro
+    of its own (OCTMPS_REF_ARCH 350): same 600-thread blocks, same settings.
+
 The kernel's source, its arithmetic and every other line are unchanged.
 
     python baseline/patch_ref.py <reference tree> <out dir>
@@ -50,6 +58,22 @@ def patch_main(src):
     return src
 
 
+ARCH_DEFINE = "#define __CUDA_ARCH__ 350 //mrei\n"
+
+
+def patch_kernel_h(src):
+    if src.count(ARCH_DEFINE) != 1:
+        raise SystemExit("patch anchor not found exactly once: the __CUDA_ARCH__ define")
+    src = src.replace(ARCH_DEFINE, "#define OCTMPS_REF_ARCH 350\n")
+    head, sep, rest = src.partition("#define OCTMPS_REF_ARCH 350\n")
+    # the tests of the setting below the define (the _WIN32 branch is left alone)
+    rest = rest.replace("#ifndef __CUDA_ARCH__", "#ifndef OCTMPS_REF_ARCH")
+    rest = rest.replace("#if __CUDA_ARCH__ ==", "#if OCTMPS_REF_ARCH ==")
+    rest = rest.replace("#elif __CUDA_ARCH__ ==", "#elif OCTMPS_REF_ARCH ==")
+    rest = rest.replace("(__CUDA_ARCH__ ==", "(OCTMPS_REF_ARCH ==")
+    return head + sep + rest
+
+
 def main():
     tree, out = sys.argv[1], sys.argv[2]
     os.makedirs(out, exist_ok=True)
@@ -59,8 +83,17 @@ def main():
     p = os.path.join(out, "main.cu")
     with open(p) as f:
         src = f.read()
+    cc_test = "if (cc[i] >= __CUDA_ARCH__) {"
+    if src.count(cc_test) != 1:
+        raise SystemExit("patch anchor not found exactly once: the compute-capability test")
+    src = src.replace(cc_test, "if (cc[i] >= OCTMPS_REF_ARCH) {")
     with open(p, "w") as f:
         f.write(patch_main(src))
+    p = os.path.join(out, "octmps_kernel.h")
+    with open(p) as f:
+        src = f.read()
+    with open(p, "w") as f:
+        f.write(patch_kernel_h(src))
 
 
 if __name__ == "__main__":

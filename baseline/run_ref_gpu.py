@@ -85,15 +85,16 @@ def run(first=96, ascans=4, photons=1_000_000, seed=1, timeout_s=900):
     os.symlink(SAFEPRIMES, os.path.join(work, "safeprimes_base32.txt"))
     env = dict(os.environ, OCTMPS_REF_MESH_CACHE=cache_bin)
     t0 = time.time()
-    r = subprocess.run(["timeout", "-k", "30", str(timeout_s), BINARY, f"-S{seed}", p["opt"],
-                        p["mesh"], p["mci"]], cwd=work, env=env, capture_output=True, text=True)
+    r = subprocess.run(["timeout", "-k", "30", str(timeout_s), "stdbuf", "-oL", BINARY,
+                        f"-S{seed}", p["opt"], p["mesh"], p["mci"]],
+                       cwd=work, env=env, capture_output=True, text=True)
     wall = time.time() - t0
     loops = [(float(m.group(1)), int(m.group(2))) for m in
              re.finditer(r"kernel loop: ([0-9.]+) ms, (\d+) launches", r.stdout)]
     sims = [float(m.group(1)) for m in re.finditer(r">>>>>>Simulation time: ([0-9.]+)", r.stdout)]
     if r.returncode != 0 or len(loops) != len(sel):
         return {"unavailable": f"reference run failed (rc {r.returncode}, {len(loops)} of "
-                               f"{len(sel)} A-scans): {(r.stderr or r.stdout)[-300:]}"}
+                               f"{len(sel)} A-scans): {(r.stderr + r.stdout)[-400:]}"}
     loop_ms = sum(ms for ms, _ in loops)
     return {
         "value": photons * len(sel) / (loop_ms / 1e3), "unit": "packets/s",
