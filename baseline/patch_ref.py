@@ -16,6 +16,14 @@ committed) and applies the measurement patches of its CUDA build:
     the build crashes at run time.  The same selection is made through a macro
     of its own (OCTMPS_REF_ARCH 350): same 600-thread blocks, same settings.
 
+  * RunGPUi fills the device arrays rootIdx and rootIdx_cont (n_threads
+    words each) by copying n_threads words from the address of the single
+    host word hstate->rootIdx (src/main.cu:309, 327): a read far past the
+    end of a small heap block, which faults on this host.  The copies come
+    from a host buffer holding the root index n_threads times (what the code
+    evidently means; InitThreadState overwrites both arrays per thread
+    anyway, src/octmps_kernel.cuh:1119-1122).
+
 The kernel's source, its arithmetic and every other line are unchanged.
 
     python baseline/patch_ref.py <reference tree> <out dir>
@@ -31,7 +39,28 @@ LAUNCH = "        OCTMPSKernel << < dimGrid, dimBlock >> > (DeviceMem, tstates);
 DONE = '    printf("[GPU %u] simulation done!\\n", hstate->dev_id);\n'
 
 
+ROOT_COPY = "    checkCudaErrors(cudaMemcpy(d_rootIdx, h_rootIdx, size,\n"
+ROOT_COPY_CONT = "    checkCudaErrors(cudaMemcpy(d_rootIdx_cont, h_rootIdx, size,\n"
+PHOTON_SECTION = "    // photon structure\n"
+
+
+def patch_root_copies(src):
+    for anchor in (ROOT_COPY, ROOT_COPY_CONT, PHOTON_SECTION):
+        if src.count(anchor) != 1:
+            raise SystemExit(f"patch anchor not found exactly once: {anchor!r}")
+    src = src.replace(ROOT_COPY, (
+        "    UINT32 *octmps_roots = (UINT32 *) malloc(size);\n"
+        "    for (UINT32 octmps_i = 0; octmps_i < n_threads; ++octmps_i)\n"
+        "        octmps_roots[octmps_i] = *h_rootIdx;\n"
+        "    checkCudaErrors(cudaMemcpy(d_rootIdx, octmps_roots, size,\n"))
+    src = src.replace(ROOT_COPY_CONT,
+                      "    checkCudaErrors(cudaMemcpy(d_rootIdx_cont, octmps_roots, size,\n")
+    src = src.replace(PHOTON_SECTION, "    free(octmps_roots);\n" + PHOTON_SECTION)
+    return src
+
+
 def patch_main(src):
+    src = patch_root_copies(src)
     for anchor in (LOOP, LAUNCH, DONE):
         if src.count(anchor) != 1:
             raise SystemExit(f"patch anchor not found exactly once: {anchor!r}")
