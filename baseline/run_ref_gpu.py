@@ -94,7 +94,8 @@ def run(first=96, ascans=4, photons=1_000_000, seed=1, timeout_s=900):
     sims = [float(m.group(1)) for m in re.finditer(r">>>>>>Simulation time: ([0-9.]+)", r.stdout)]
     if r.returncode != 0 or len(loops) != len(sel):
         return {"unavailable": f"reference run failed (rc {r.returncode}, {len(loops)} of "
-                               f"{len(sel)} A-scans): {(r.stderr + r.stdout)[-400:]}"}
+                               f"{len(sel)} A-scans): stderr: {r.stderr[-400:]!r} stdout: "
+                               f"{r.stdout[-200:]!r}"}
     loop_ms = sum(ms for ms, _ in loops)
     return {
         "value": photons * len(sel) / (loop_ms / 1e3), "unit": "packets/s",
