@@ -104,7 +104,7 @@ def run(first=96, ascans=4, photons=1_000_000, seed=1, timeout_s=900):
         "launches": [n for _, n in loops],
         "wall_timer_packets_per_s": photons * len(sel) / (sum(sims) / 1e3) if sims else None,
         "process_s": wall, "lanes": LANES, "seed": seed,
-        "build": "reference sources, nvcc --use_fast_math -O3 -maxrregcount=104 sm_100a; "
+        "build": "reference sources, nvcc --use_fast_math -O3 -maxrregcount=96 sm_100a; "
                  "patches: event timing around the relaunch loop, relaunch cap; mesh from the "
                  "reference's MeshGraph (cached)",
         "timing": "cudaEvents around RunGPUi's relaunch loop of OCTMPSKernel, summed over the "
