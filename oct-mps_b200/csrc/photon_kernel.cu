@@ -225,8 +225,13 @@ struct Lane {
     const RegionConst<T> *regions;
     const void *planes;
     const int4 *adj;
-    T px, py, pz;
-    int32_t type_bias;
+    // The probe position and bias type are read from the job descriptor
+    // where they are used (launches, biased scatterings, exits): held in
+    // registers across the step loop they were spilled to local memory.
+    __device__ __forceinline__ T px() const { return (T)__ldg(&jd->probe_x); }
+    __device__ __forceinline__ T py() const { return (T)__ldg(&jd->probe_y); }
+    __device__ __forceinline__ T pz() const { return (T)__ldg(&jd->probe_z); }
+    __device__ __forceinline__ int32_t type_bias() const { return __ldg(&jd->type_bias); }
     // record of the current packet (kRecord only)
     unsigned long long rhash;
     uint32_t rsteps, rhits, rscatters, rrestores, rdetections, rsurvivals;
@@ -236,21 +241,27 @@ struct Lane {
     __device__ __forceinline__ T rand_co_R() { return DevNum<T>::rand_value(mwc_next(xR, aR)); }
     __device__ __forceinline__ T rand_co_S() { return DevNum<T>::rand_value(mwc_next(xS, aS)); }
 
+    // The current region's n, mu_t and 1/mu_t stay in registers (every step
+    // uses them); mu_a/mu_t and g are read where a scattering uses them.
     __device__ __forceinline__ void load_region(int r) {
         const T *p = reinterpret_cast<const T *>(regions + r);
         rg.n = __ldg(p + 0);
         rg.muas = __ldg(p + 1);
         rg.rmuas = __ldg(p + 2);
-        rg.mua_muas = __ldg(p + 3);
-        rg.g = __ldg(p + 4);
         region = r;
+    }
+    __device__ __forceinline__ T region_mua_muas() const {
+        return __ldg(reinterpret_cast<const T *>(regions + region) + 3);
+    }
+    __device__ __forceinline__ T region_g() const {
+        return __ldg(reinterpret_cast<const T *>(regions + region) + 4);
     }
 
     // LaunchPhoton, src/octmps_kernel.cuh:475-503.
     __device__ __forceinline__ void launch() {
-        x = px;
-        y = py;
-        z = pz;
+        x = px();
+        y = py();
+        z = pz();
         ux = 0;
         uy = 0;
         uz = 1;
@@ -332,7 +343,7 @@ struct Lane {
     // SpinBias, src/octmps_kernel.cuh:898-1086.
     __device__ void spin_bias(SplitCopy<T, P> &cont) {
         const JobDesc &J = *jd;
-        const T g = rg.g;
+        const T g = region_g();
         const T g2 = g * g;
         T ax = ux, ay = uy, az = uz;
         const T ox = ux, oy = uy, oz = uz;
@@ -359,9 +370,9 @@ struct Lane {
             btmp = (T)J.bias_a;
             first = true;
         }
-        T vx = px - x;
-        T vy = py - y;
-        T vz = pz - z;
+        T vx = px() - x;
+        T vy = py() - y;
+        T vz = pz() - z;
         const T len = sqrtT(DevNum<T>::mad(vz, vz, DevNum<T>::mad(vx, vx, vy * vy)));
         if (kFused<T>) {
             const T rl = rcpT(len);  // FP32 forms: one reciprocal, three products
@@ -584,12 +595,13 @@ struct Lane {
                 ev = 4;
                 if (uz < (T)0) {
                     bool filt = false;
-                    const T dx = x - px;
-                    const T dy = y - py;
+                    const T dx = x - px();
+                    const T dy = y - py();
                     const T rr = sqrtT(DevNum<T>::mad(dx, dx, dy * dy));
                     if (rr < (T)jd->radius && -uz > (T)jd->cos_collect) {
-                        if (type_bias == 0 || type_bias == 3) filt = true;
-                        if ((fst_flag && type_bias == 37) || (loc_fst == max_depth && type_bias != 37) ||
+                        const int32_t tb = type_bias();
+                        if (tb == 0 || tb == 3) filt = true;
+                        if ((fst_flag && tb == 37) || (loc_fst == max_depth && tb != 37) ||
                             num_back > 0)
                             filt = true;
                     }
@@ -633,10 +645,11 @@ struct Lane {
     __device__ __forceinline__ bool phase_b(SplitCopy<T, P> &cont) {
         if (kRecord) ++rscatters;
         // Drop, :584-588
-        w = DevNum<T>::mad(-w, rg.mua_muas, w);
-        if (type_bias == 0) {
-            rotate(spin_theta(rg.g), ux, uy, uz, false);
-        } else if (type_bias == 37) {
+        w = DevNum<T>::mad(-w, region_mua_muas(), w);
+        const int32_t tb = type_bias();
+        if (tb == 0) {
+            rotate(spin_theta(region_g()), ux, uy, uz, false);
+        } else if (tb == 37) {
             spin_bias(cont);
         }
         return finish(1, cont);
@@ -652,7 +665,7 @@ struct Lane {
                 w *= DevNum<T>::div((T)1, DevNum<T>::chance);
                 ev |= 16;
                 if (kRecord) ++rsurvivals;
-            } else if (fst_flag && type_bias != 3) {
+            } else if (fst_flag && type_bias() != 3) {
                 const T lr_tmp = lr_after;
                 x = cont.x;
                 y = cont.y;
@@ -670,11 +683,11 @@ struct Lane {
                 loc_fst = -1;
                 sleft = 0;
                 if (cont.region != region) load_region(cont.region);
-                rotate(spin_theta(rg.g), ux, uy, uz, false);
+                rotate(spin_theta(region_g()), ux, uy, uz, false);
                 lr = lr_tmp < (T)1 ? (T)1 - lr_tmp : (T)1;
                 ev |= 32;
                 if (kRecord) ++rrestores;
-                restores_++;
+                atomicAdd(&jd->stats[1], 1ull);  // split copies resumed (rare)
                 stall = 0;
             } else {
                 ev |= 64;
@@ -687,7 +700,6 @@ struct Lane {
         }
         return end;
     }
-    uint32_t restores_;
     uint32_t stall;  // consecutive boundary hits that did not move the photon
 };
 
@@ -701,7 +713,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     Lane<T, P, kRecord> L;
     L.jd = nullptr;
     L.region = -1;
-    L.restores_ = 0;
     // packets still to run in the current unit (the runtime keeps a job's
     // packets per lane below 2^32) and steps of the current packet (capped
     // at step_cap <= 2^32)
@@ -823,10 +834,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
                     L.regions = reinterpret_cast<const RegionConst<T> *>(jd->regions);
                     L.planes = jd->planes;
                     L.adj = reinterpret_cast<const int4 *>(jd->adj);
-                    L.px = (T)jd->probe_x;
-                    L.py = (T)jd->probe_y;
-                    L.pz = (T)jd->probe_z;
-                    L.type_bias = jd->type_bias;
                     L.region = -1;
                 }
                 L.xG = jd->rng_x[v];
@@ -913,10 +920,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
         if (done) {
             // per-packet statistics: steps, split copies resumed, packets
             atomicAdd(&L.jd->stats[0], (unsigned long long)steps_packet);
-            if (L.restores_) atomicAdd(&L.jd->stats[1], (unsigned long long)L.restores_);
             atomicAdd(&L.jd->stats[2], 1ull);
-            L.restores_ = 0;
-            if (kRecord && recording) {
+                    if (kRecord && recording) {
                 PacketRecordDev r;
                 r.hash = L.rhash;
                 r.x = L.xG;
@@ -1084,10 +1089,6 @@ __device__ __forceinline__ void unpack(const uint32_t *w, const LaunchArgs &args
     L.regions = reinterpret_cast<const RegionConst<T> *>(jd->regions);
     L.planes = jd->planes;
     L.adj = reinterpret_cast<const int4 *>(jd->adj);
-    L.px = (T)jd->probe_x;
-    L.py = (T)jd->probe_y;
-    L.pz = (T)jd->probe_z;
-    L.type_bias = jd->type_bias;
     L.x = get_w<T>(w, 0 * t);
     L.y = get_w<T>(w, 1 * t);
     L.z = get_w<T>(w, 2 * t);
@@ -1113,7 +1114,6 @@ __device__ __forceinline__ void unpack(const uint32_t *w, const LaunchArgs &args
     L.aG = m.aG;
     L.aR = m.aR;
     L.aS = m.aS;
-    L.restores_ = 0;
     if constexpr (kRecord) {
         constexpr int R = Lay::REC;
         L.rhash = get_w<unsigned long long>(w, R);
@@ -1212,10 +1212,6 @@ __device__ __forceinline__ bool start_unit(const LaunchArgs &args, unsigned long
     L.regions = reinterpret_cast<const RegionConst<T> *>(jd->regions);
     L.planes = jd->planes;
     L.adj = reinterpret_cast<const int4 *>(jd->adj);
-    L.px = (T)jd->probe_x;
-    L.py = (T)jd->probe_y;
-    L.pz = (T)jd->probe_z;
-    L.type_bias = jd->type_bias;
     L.region = -1;
     L.xG = jd->rng_x[v];
     L.xR = jd->rng_xR[v];
@@ -1223,7 +1219,6 @@ __device__ __forceinline__ bool start_unit(const LaunchArgs &args, unsigned long
     L.aG = m.aG;
     L.aR = m.aR;
     L.aS = m.aS;
-    L.restores_ = 0;
     L.launch();
     L.draw_step();
     return true;
@@ -1393,7 +1388,6 @@ __global__ void __launch_bounds__(kPoolBlock, kMinBlocks)
                 if (r == kPending) step_done = false;
                 else end = r == kEnd;
             }
-            if (L.restores_) atomicAdd(&L.jd->stats[1], (unsigned long long)L.restores_);
             if (!step_done) {
                 to = 2;
             } else {
