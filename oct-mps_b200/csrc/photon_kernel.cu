@@ -31,10 +31,10 @@ namespace {
 
 constexpr int kBlock = 256;
 
-// Outcomes of the first half of a step.
-constexpr int kDone = 0;     // step finished, packet continues
-constexpr int kEnd = 1;      // step finished, packet ended
-constexpr int kPending = 2;  // no face reached: scattering still to do
+// Results of a half-step besides its event code (>= 1): no face reached, the
+// scattering half still to do; or the packet ended on an error.
+constexpr int kEvPending = -1;
+constexpr int kEvError = -2;
 
 template <typename T>
 struct Plane4;
@@ -448,11 +448,6 @@ struct Lane {
         }
     }
 
-    // First half of a propagation step, OCTMPSKernel's loop body
-    // (src/octmps_kernel.cuh:1351-1392): step size, boundary test, hop and,
-    // when a face is reached, reflection or transmission and the roulette.
-    // Returns kDone, kEnd (the packet ended) or kPending (no face reached:
-    // the step continues in phase_b).
     // ComputeStepSize's draw for a step that starts with sleft == 0,
     // src/octmps_kernel.cuh:505-515.  The kernels draw it at the end of the
     // previous step (after its roulette and stop checks) or at the launch:
@@ -463,8 +458,14 @@ struct Lane {
         s_next = -log_method(r) * rg.rmuas;
     }
 
+    // First half of a propagation step, OCTMPSKernel's loop body
+    // (src/octmps_kernel.cuh:1351-1392): step size, boundary test, hop and,
+    // when a face is reached, reflection or transmission.  Returns the event
+    // code for finish() (the roulette, called once per step by the loop),
+    // kEvPending when no face was reached (the step continues in half_b) or
+    // kEvError.
     template <bool kDrawnAhead = false>
-    __device__ __forceinline__ int phase_a(SplitCopy<T, P> &cont, unsigned int *err) {
+    __device__ __forceinline__ int half_a(SplitCopy<T, P> &cont, unsigned int *err) {
         int ev = 0;
         // ComputeStepSize, :505-515
         if (sleft == (T)0) {
@@ -540,7 +541,7 @@ struct Lane {
         if (hit) {
             if (face < 0) {
                 atomicOr(err, kErrNoExitFace);
-                return kEnd;
+                return kEvError;
             }
             // FastReflectTransmit, :590-775
             if (kRecord) ++rhits;
@@ -634,15 +635,14 @@ struct Lane {
                 ev = 3;
             }
         } else {
-            return kPending;  // the scattering half of the step runs in phase_b
+            return kEvPending;  // the scattering half of the step runs in half_b
         }
-        return finish(ev, cont) ? kEnd : kDone;
+        return ev;
     }
 
     // Second half of a step that did not reach a face: Drop, then Spin or
-    // SpinBias (:1359-1369), then the roulette.  Returns true when the
-    // packet ends.
-    __device__ __forceinline__ bool phase_b(SplitCopy<T, P> &cont) {
+    // SpinBias (:1359-1369).  Returns the event code for finish().
+    __device__ __forceinline__ int half_b(SplitCopy<T, P> &cont) {
         if (kRecord) ++rscatters;
         // Drop, :584-588
         w = DevNum<T>::mad(-w, region_mua_muas(), w);
@@ -652,7 +652,7 @@ struct Lane {
         } else if (tb == 37) {
             spin_bias(cont);
         }
-        return finish(1, cont);
+        return 1;
     }
 
     // Roulette, :1376-1392, and the step's record.  Returns true when the
@@ -866,20 +866,21 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
         const bool run_b = ready == 0u || __popc(pend) * 32 >= share * __popc(live);
         if ((pend | ready) == 0u) __nanosleep(kIdleSleepNs);  // every live lane waits for work
         if (idle) continue;
-        bool end;
+        int ev;
         if (run_b) {
             if (!pending) continue;
             pending = false;
-            end = L.phase_b(cont);
+            ev = L.half_b(cont);
         } else {
             if (pending) continue;
-            const int r = L.template phase_a<true>(cont, err);
-            if (r == kPending) {
+            ev = L.template half_a<true>(cont, err);
+            if (ev == kEvPending) {
                 pending = true;
                 continue;
             }
-            end = r == kEnd;
         }
+        // one roulette call site for both halves (its code inlined once)
+        const bool end = ev == kEvError || L.finish(ev, cont);
         ++steps_packet;
         bool done = end;
         // A packet is stopped (its split copy too) at the step cap, an
@@ -1380,14 +1381,9 @@ __global__ void __launch_bounds__(kPoolBlock, kMinBlocks)
         int to = 0;  // 0: leaves the pool, 1: stack A, 2: stack B
         if (active) {
             SplitCopy<T, P> &cont = wsplit[m.home];
-            bool end = false, step_done = true;
-            if (run_b) {
-                end = L.phase_b(cont);
-            } else {
-                const int r = L.template phase_a<true>(cont, err);
-                if (r == kPending) step_done = false;
-                else end = r == kEnd;
-            }
+            const int ev = run_b ? L.half_b(cont) : L.template half_a<true>(cont, err);
+            const bool step_done = ev != kEvPending;
+            const bool end = step_done && (ev == kEvError || L.finish(ev, cont));
             if (!step_done) {
                 to = 2;
             } else {
