@@ -25,6 +25,7 @@
 
 #include "kernel_iface.h"
 #include "octmps_host.h"
+#include "region_consts.h"
 
 using namespace octmps;
 
@@ -81,14 +82,6 @@ __global__ void validate_adj(const int32_t *adj, int64_t n, int32_t n_tets, int3
     }
 }
 
-double div_rd_host(double a, double b) {
-    double q = a / b;
-    if (!std::isfinite(q) || q == 0.0) return q;
-    double r = std::fma(-q, b, a);
-    if (r != 0.0 && ((r < 0.0) == (b > 0.0))) q = std::nextafter(q, -INFINITY);
-    return q;
-}
-
 }  // namespace
 
 static_assert(OCTMPS_NOALLOC_TALLY_BYTES(600) == 32 + 2 * 4816 + 6 * 4816,
@@ -118,17 +111,8 @@ extern "C" octmps_status octmps_ascan_run_noalloc(const octmps_noalloc_ascan *a,
     // Host image of the scratch area (stack memory; no allocation).
     unsigned char img[kScratchBytes];
     memset(img, 0, sizeof img);
-    RegionConst<float> *rg = reinterpret_cast<RegionConst<float> *>(img + kRegionOff);
-    for (int i = 0; i < s.n_regions; ++i) {
-        // read_simulation_data (src/octmps_io.cpp:625-626) and
-        // InitDeviceConstantMemory (src/octmps_kernel.cuh:204-214).
-        const double mutr = 1.0 / (s.regions[i].mua + s.regions[i].mus);
-        rg[i].n = (float)s.regions[i].n;
-        rg[i].muas = (float)(1.0 / mutr);
-        rg[i].rmuas = (float)mutr;
-        rg[i].mua_muas = (float)(s.regions[i].mua * mutr);
-        rg[i].g = (float)s.regions[i].g;
-    }
+    // the region constants as octmps_job_submit derives them (region_consts.h)
+    fill_region_consts<float>(s, reinterpret_cast<RegionConst<float> *>(img + kRegionOff));
     JobDesc D;
     memset(&D, 0, sizeof D);
     D.planes = a->planes;
@@ -160,8 +144,8 @@ extern "C" octmps_status octmps_ascan_run_noalloc(const octmps_noalloc_ascan *a,
     D.rnd_step = s.rnd_step_size_in_tissue;
     D.n_ambient = s.regions[0].n;
     D.shift = s.optical_depth_shift;
-    D.bin_width = div_rd_host(s.coherence_length_source, 6.0);
-    D.half_lc = div_rd_host(s.coherence_length_source, 2.0);
+    D.bin_width = div_rd(s.coherence_length_source, 6.0);
+    D.half_lc = div_rd(s.coherence_length_source, 2.0);
     D.root_tet = a->root_tet;
     D.root_region = a->root_region;
     D.n_regions = s.n_regions;

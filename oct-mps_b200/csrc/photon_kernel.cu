@@ -70,12 +70,50 @@ struct Plane4<double> {
     }
 };
 
+// A photon's split copy: its state at the first biased scattering toward the
+// probe (src/octmps_kernel.cuh:933-951), resumed when the photon dies
+// (:1376-1392).  save() stores a lane's state, restore() puts it back (all
+// but the region, which it returns).  The per-lane kernel keeps one record
+// per thread in shared memory, the pooled kernel one per photon in global
+// memory.
 template <typename T, typename P>
 struct SplitCopy {
     T x, y, z, ux, uy, uz, w, max_depth, lr;
     P op;
     int32_t tet, region;
     uint32_t num_back;
+    template <class L>
+    __device__ __forceinline__ void save(const L &l) {
+        x = l.x;
+        y = l.y;
+        z = l.z;
+        ux = l.ux;
+        uy = l.uy;
+        uz = l.uz;
+        w = l.w;
+        max_depth = l.max_depth;
+        lr = l.lr;
+        op = l.op;
+        tet = l.tet;
+        region = l.region;
+        num_back = l.num_back;
+    }
+    template <class L>
+    __device__ __forceinline__ int32_t restore(L &l) const {
+        l.x = x;
+        l.y = y;
+        l.z = z;
+        l.ux = ux;
+        l.uy = uy;
+        l.uz = uz;
+        l.w = w;
+        l.max_depth = max_depth;
+        l.lr = lr;
+        l.op = op;
+        l.tet = tet;
+        l.num_back = num_back;
+        return region;
+    }
 };
 
 struct PacketRecordDev {
@@ -242,20 +280,15 @@ struct Lane {
     __device__ __forceinline__ T rand_co_S() { return DevNum<T>::rand_value(mwc_next(xS, aS)); }
 
     // The current region's n, mu_t and 1/mu_t stay in registers (every step
-    // uses them); mu_a/mu_t and g are read where a scattering uses them.
+    // uses them); its other constants are read where a scattering uses them.
     __device__ __forceinline__ void load_region(int r) {
-        const T *p = reinterpret_cast<const T *>(regions + r);
-        rg.n = __ldg(p + 0);
-        rg.muas = __ldg(p + 1);
-        rg.rmuas = __ldg(p + 2);
+        const RegionConst<T> *c = regions + r;
+        rg.n = __ldg(&c->n);
+        rg.muas = __ldg(&c->muas);
+        rg.rmuas = __ldg(&c->rmuas);
         region = r;
     }
-    __device__ __forceinline__ T region_mua_muas() const {
-        return __ldg(reinterpret_cast<const T *>(regions + region) + 3);
-    }
-    __device__ __forceinline__ T region_g() const {
-        return __ldg(reinterpret_cast<const T *>(regions + region) + 4);
-    }
+    __device__ __forceinline__ const RegionConst<T> *rc() const { return regions + region; }
 
     // LaunchPhoton, src/octmps_kernel.cuh:475-503.
     __device__ __forceinline__ void launch() {
@@ -285,31 +318,39 @@ struct Lane {
         }
     }
 
-    // SpinTheta, src/octmps_kernel.cuh:807-820.
-    __device__ __forceinline__ T spin_theta(T g) {
+    // SpinTheta, src/octmps_kernel.cuh:807-820, with the current region's g:
+    // temp = (1 - g^2) / (1 + 2 g r - g), cost = (1 + g^2 - temp^2) / 2g, the
+    // terms in g from the region constants.
+    __device__ __forceinline__ T spin_theta() {
+        const RegionConst<T> *c = rc();
         T cost;
-        if (g == (T)0) {
+        if (__ldg(&c->g) == (T)0) {
             cost = (T)2 * ((T)1 - rand_co_S()) - (T)1;
         } else {
             const T r = (T)1 - rand_co_S();
-            const T temp = DevNum<T>::div(DevNum<T>::mad(-g, g, (T)1), DevNum<T>::mad(g + g, r, (T)1 - g));
-            cost = DevNum<T>::div(DevNum<T>::mad(-temp, temp, DevNum<T>::mad(g, g, (T)1)), g + g);
+            const T g_2x = __ldg(&c->g_2x);
+            const T temp = DevNum<T>::div(__ldg(&c->g_1m2f), DevNum<T>::mad(g_2x, r, __ldg(&c->g_1m)));
+            cost = DevNum<T>::div(DevNum<T>::mad(-temp, temp, __ldg(&c->g_1p2)), g_2x);
             if (cost < (T)-1) cost = -1;
             else if (cost > (T)1) cost = 1;
         }
         return cost;
     }
 
-    // SpinThetaForwardFstBias, src/octmps_kernel.cuh:881-896.
-    __device__ __forceinline__ T spin_theta_forward(T g) {
+    // SpinThetaForwardFstBias, src/octmps_kernel.cuh:881-896, with the job's
+    // bias coefficient b: temp = r / (1 - b) + (1 - r) / sqrt(1 + b^2),
+    // cost = (1 + b^2 - 1 / temp^2) / 2b.
+    __device__ __forceinline__ T spin_theta_forward() {
+        const RegionConst<T> *c = rc();
+        const T b_2x = __ldg(&c->b_2x);
         T cost;
-        if (g == (T)0) {
+        if (b_2x == (T)0) {
             cost = (T)1 - rand_co_S();
         } else {
             const T r = (T)1 - rand_co_S();
-            const T temp = DevNum<T>::div(r, (T)1 - g) +
-                           DevNum<T>::div((T)1 - r, sqrtT(DevNum<T>::mad(g, g, (T)1)));
-            cost = DevNum<T>::div(DevNum<T>::mad(g, g, (T)1) - DevNum<T>::div((T)1, temp * temp), g + g);
+            const T temp = DevNum<T>::div(r, __ldg(&c->b_1m)) +
+                           DevNum<T>::div((T)1 - r, __ldg(&c->b_sq1p2));
+            cost = DevNum<T>::div(__ldg(&c->b_1p2) - DevNum<T>::div((T)1, temp * temp), b_2x);
             if (cost < (T)-1) cost = -1;
             else if (cost > (T)1) cost = 1;
         }
@@ -341,29 +382,17 @@ struct Lane {
     }
 
     // SpinBias, src/octmps_kernel.cuh:898-1086.
-    __device__ void spin_bias(SplitCopy<T, P> &cont) {
+    template <class C>
+    __device__ void spin_bias(C &cont) {
         const JobDesc &J = *jd;
-        const T g = region_g();
-        const T g2 = g * g;
+        const RegionConst<T> *c = rc();
         T ax = ux, ay = uy, az = uz;
         const T ox = ux, oy = uy, oz = uz;
         T btmp = 0;
         int reached = 0;
         bool first = false;
         if (z > (T)J.tdmin && z < (T)J.tdmax && uz > (T)0 && !fst_flag) {
-            cont.x = x;
-            cont.y = y;
-            cont.z = z;
-            cont.ux = ux;
-            cont.uy = uy;
-            cont.uz = uz;
-            cont.w = w;
-            cont.max_depth = max_depth;
-            cont.lr = lr;
-            cont.op = op;
-            cont.tet = tet;
-            cont.region = region;
-            cont.num_back = num_back;
+            cont.save(*this);
             reached = 1;
             fst_flag = 1;
             loc_fst = z;
@@ -386,10 +415,9 @@ struct Lane {
         }
         if ((fst_flag || num_back > 0) && !reached) {
             reached = 2;
-            // -log(0)/mu_t is +infinity: with rndStepSizeInTissue = 0 the
-            // distance test always holds.
-            const T rs = (T)J.rnd_step;
-            const bool far = rs == (T)0 || DevNum<T>::div(-log_method(rs), rg.muas) >= len;
+            // -log(rndStepSizeInTissue) / mu_t from the region constants
+            // (+infinity for a step of 0: the distance test always holds)
+            const bool far = __ldg(&c->far) >= len;
             if (far && -vz >= (T)J.cos_collect) reached = 1;
             btmp = (T)J.bias_a;
         }
@@ -399,15 +427,15 @@ struct Lane {
         if (reached) {
             sel = rand_co_S() <= pb ? 1 : 2;
             if (reached == 1 || sel == 1) {
-                cost = spin_theta_forward(btmp);
+                cost = spin_theta_forward();
                 ax = vx;
                 ay = vy;
                 az = vz;
             } else {
-                cost = spin_theta(g);
+                cost = spin_theta();
             }
         } else {
-            cost = spin_theta(g);
+            cost = spin_theta();
         }
         cost = fmaxT(cost, (T)-1);
         cost = fminT(cost, (T)1);
@@ -424,24 +452,23 @@ struct Lane {
             costg1 = fminT(fmaxT(costg1, (T)-1), (T)1);
         }
         if (btmp != (T)0) {
-            const T opa2 = DevNum<T>::mad(btmp, btmp, (T)1);
-            const T sq_opa2 = sqrtT(opa2);
+            // b = btmp (the job's coefficient); the terms in b and g alone
+            // come from the region constants
             T f;
             if (reached == 1) {
-                const T b1 = opa2 - (btmp + btmp) * cost;
-                const T h1 = DevNum<T>::mad(g, g, (T)1) - (g + g) * costg;
-                const T num = ((T)1 - g2) * (sq_opa2 - (T)1 + btmp) * sqrtT(b1 * b1 * b1);
-                const T den = (btmp + btmp) * ((T)1 - btmp) * sq_opa2 * sqrtT(h1 * h1 * h1);
+                const T b1 = __ldg(&c->b_1p2) - __ldg(&c->b_2x) * cost;
+                const T h1 = __ldg(&c->g_1p2) - __ldg(&c->g_2x) * costg;
+                const T num = __ldg(&c->g_1m2) * __ldg(&c->b_c1) * sqrtT(b1 * b1 * b1);
+                const T den = __ldg(&c->b_d1) * sqrtT(h1 * h1 * h1);
                 f = DevNum<T>::div(num, den);
             } else {
                 const T c1 = sel == 1 ? cost : costg1;
                 const T c2 = sel == 1 ? costg : cost;
-                const T b1 = opa2 - (btmp + btmp) * c1;
-                const T pdf1 = DevNum<T>::div(sq_opa2 * btmp * ((T)1 - btmp),
-                                              (sq_opa2 - (T)1 + btmp) * sqrtT(b1 * b1 * b1));
-                const T h2 = sqrtT(DevNum<T>::mad(g, g, (T)1) - (g + g) * c2);
-                const T pdf2 = DevNum<T>::div((T)1 - g2, (T)2 * (h2 * h2 * h2));
-                f = DevNum<T>::div(pdf2, DevNum<T>::mad(pb, pdf1, ((T)1 - pb) * pdf2));
+                const T b1 = __ldg(&c->b_1p2) - __ldg(&c->b_2x) * c1;
+                const T pdf1 = DevNum<T>::div(__ldg(&c->b_p1), __ldg(&c->b_c1) * sqrtT(b1 * b1 * b1));
+                const T h2 = sqrtT(__ldg(&c->g_1p2) - __ldg(&c->g_2x) * c2);
+                const T pdf2 = DevNum<T>::div(__ldg(&c->g_1m2), (T)2 * (h2 * h2 * h2));
+                f = DevNum<T>::div(pdf2, DevNum<T>::mad(pb, pdf1, __ldg(&c->pb_1m) * pdf2));
             }
             lr *= f;
             if (first) lr_after = lr;
@@ -465,7 +492,7 @@ struct Lane {
     // kEvPending when no face was reached (the step continues in half_b) or
     // kEvError.
     template <bool kDrawnAhead = false>
-    __device__ __forceinline__ int half_a(SplitCopy<T, P> &cont, unsigned int *err) {
+    __device__ __forceinline__ int half_a(unsigned int *err) {
         int ev = 0;
         // ComputeStepSize, :505-515
         if (sleft == (T)0) {
@@ -548,8 +575,9 @@ struct Lane {
             const T ca1 = -min_cos;
             const int32_t entry = face == 0 ? nb.x : face == 1 ? nb.y : face == 2 ? nb.z : nb.w;
             const int next_region = entry < 0 ? 0 : (int)((uint32_t)entry >> kAdjIndexBits);
-            const T nt = entry < 0 ? (T)jd->n_ambient
-                                   : __ldg(reinterpret_cast<const T *>(regions + next_region));
+            const T nt = entry < 0                ? (T)jd->n_ambient
+                         : next_region == region ? rg.n
+                                                 : __ldg(&regions[next_region].n);
             T r;
             const T sa1_sq = DevNum<T>::mad(-ca1, ca1, (T)1);
             if (kFused<T> && rg.n == nt) {
@@ -642,13 +670,14 @@ struct Lane {
 
     // Second half of a step that did not reach a face: Drop, then Spin or
     // SpinBias (:1359-1369).  Returns the event code for finish().
-    __device__ __forceinline__ int half_b(SplitCopy<T, P> &cont) {
+    template <class C>
+    __device__ __forceinline__ int half_b(C &cont) {
         if (kRecord) ++rscatters;
         // Drop, :584-588
-        w = DevNum<T>::mad(-w, region_mua_muas(), w);
+        w = DevNum<T>::mad(-w, __ldg(&rc()->mua_muas), w);
         const int32_t tb = type_bias();
         if (tb == 0) {
-            rotate(spin_theta(region_g()), ux, uy, uz, false);
+            rotate(spin_theta(), ux, uy, uz, false);
         } else if (tb == 37) {
             spin_bias(cont);
         }
@@ -657,7 +686,8 @@ struct Lane {
 
     // Roulette, :1376-1392, and the step's record.  Returns true when the
     // packet ends.
-    __device__ __forceinline__ bool finish(int ev, SplitCopy<T, P> &cont) {
+    template <class C>
+    __device__ __forceinline__ bool finish(int ev, C &cont) {
         bool end = false;
         if (w < DevNum<T>::weight) {
             const T rnd = rand_co_G();
@@ -667,23 +697,12 @@ struct Lane {
                 if (kRecord) ++rsurvivals;
             } else if (fst_flag && type_bias() != 3) {
                 const T lr_tmp = lr_after;
-                x = cont.x;
-                y = cont.y;
-                z = cont.z;
-                ux = cont.ux;
-                uy = cont.uy;
-                uz = cont.uz;
-                w = cont.w;
-                max_depth = cont.max_depth;
-                lr = cont.lr;
-                op = cont.op;
-                tet = cont.tet;
-                num_back = cont.num_back;
+                const int32_t cr = cont.restore(*this);
                 fst_flag = 0;
                 loc_fst = -1;
                 sleft = 0;
-                if (cont.region != region) load_region(cont.region);
-                rotate(spin_theta(region_g()), ux, uy, uz, false);
+                if (cr != region) load_region(cr);
+                rotate(spin_theta(), ux, uy, uz, false);
                 lr = lr_tmp < (T)1 ? (T)1 - lr_tmp : (T)1;
                 ev |= 32;
                 if (kRecord) ++rrestores;
@@ -708,6 +727,10 @@ struct Lane {
 template <typename T, typename P, bool kRecord, int kMinBlocks>
 __global__ void __launch_bounds__(kBlock, kMinBlocks)
     photon_kernel(const LaunchArgs args, PacketRecordDev *records) {
+    // one split copy per thread (touched only at first biased scatterings and
+    // restores, so the record layout's bank conflicts cost little; a table
+    // with one column per field measured 10 % slower: its base address is
+    // held in registers across the loop)
     __shared__ SplitCopy<T, P> cont_all[kBlock];
     SplitCopy<T, P> &cont = cont_all[threadIdx.x];
     Lane<T, P, kRecord> L;
@@ -873,7 +896,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
             ev = L.half_b(cont);
         } else {
             if (pending) continue;
-            ev = L.template half_a<true>(cont, err);
+            ev = L.template half_a<true>(err);
             if (ev == kEvPending) {
                 pending = true;
                 continue;
@@ -1381,7 +1404,7 @@ __global__ void __launch_bounds__(kPoolBlock, kMinBlocks)
         int to = 0;  // 0: leaves the pool, 1: stack A, 2: stack B
         if (active) {
             SplitCopy<T, P> &cont = wsplit[m.home];
-            const int ev = run_b ? L.half_b(cont) : L.template half_a<true>(cont, err);
+            const int ev = run_b ? L.half_b(cont) : L.template half_a<true>(err);
             const bool step_done = ev != kEvPending;
             const bool end = step_done && (ev == kEvError || L.finish(ev, cont));
             if (!step_done) {

@@ -19,17 +19,72 @@
 #ifndef OCTMPS_PHOTON_MATH_CUH
 #define OCTMPS_PHOTON_MATH_CUH
 
+#include <cmath>
 #include <cstdint>
+#include <cstring>
 
 namespace octmps {
 
-__device__ __forceinline__ float log_method(float x) {
-    if (x == 0.0f) return -__int_as_float(0x7f800000);
-    if (!(x > 0.0f) || isinf(x)) return x < 0.0f ? __int_as_float(0x7fc00000) : x;
-    uint32_t b = __float_as_uint(x);
+// Bit casts and fused multiply-adds usable on both sides: the host derives a
+// few per-job constants (region_consts.h) with the kernel's own logarithm.
+__host__ __device__ __forceinline__ uint32_t bits_of(float x) {
+#ifdef __CUDA_ARCH__
+    return __float_as_uint(x);
+#else
+    uint32_t u;
+    memcpy(&u, &x, sizeof u);
+    return u;
+#endif
+}
+__host__ __device__ __forceinline__ float float_of(uint32_t u) {
+#ifdef __CUDA_ARCH__
+    return __uint_as_float(u);
+#else
+    float x;
+    memcpy(&x, &u, sizeof x);
+    return x;
+#endif
+}
+__host__ __device__ __forceinline__ uint64_t bits_of(double x) {
+#ifdef __CUDA_ARCH__
+    return (uint64_t)__double_as_longlong(x);
+#else
+    uint64_t u;
+    memcpy(&u, &x, sizeof u);
+    return u;
+#endif
+}
+__host__ __device__ __forceinline__ double double_of(uint64_t u) {
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double((long long)u);
+#else
+    double x;
+    memcpy(&x, &u, sizeof x);
+    return x;
+#endif
+}
+__host__ __device__ __forceinline__ float fma_rn(float a, float b, float c) {
+#ifdef __CUDA_ARCH__
+    return __fmaf_rn(a, b, c);
+#else
+    return std::fma(a, b, c);
+#endif
+}
+__host__ __device__ __forceinline__ double fma_rn(double a, double b, double c) {
+#ifdef __CUDA_ARCH__
+    return __fma_rn(a, b, c);
+#else
+    return std::fma(a, b, c);
+#endif
+}
+
+__host__ __device__ __forceinline__ float log_method(float x) {
+    if (x == 0.0f) return -float_of(0x7f800000u);
+    if (!(x > 0.0f) || std::isinf(x)) return x < 0.0f ? float_of(0x7fc00000u) : x;
+    uint32_t b = bits_of(x);
     int e = 0;
     if (b < 0x00800000u) {
-        b = __float_as_uint(x * 0x1p23f);
+        b = bits_of(x * 0x1p23f);
         e = -23;
     }
     e += (int)(b >> 23) - 127;
@@ -38,26 +93,26 @@ __device__ __forceinline__ float log_method(float x) {
         mb -= 0x00800000u;
         e += 1;
     }
-    const float m = __uint_as_float(mb);
+    const float m = float_of(mb);
     const float f = m - 1.0f;
     const float s = f / (2.0f + f);
     const float z = s * s;
     const float t = s + s;
-    float p = __fmaf_rn(z, 0x1.c71c72p-4f, 0x1.24924ap-3f);
-    p = __fmaf_rn(z, p, 0x1.99999ap-3f);
-    p = __fmaf_rn(z, p, 0x1.555556p-2f);
-    const float lm = __fmaf_rn(t * z, p, t);
+    float p = fma_rn(z, 0x1.c71c72p-4f, 0x1.24924ap-3f);
+    p = fma_rn(z, p, 0x1.99999ap-3f);
+    p = fma_rn(z, p, 0x1.555556p-2f);
+    const float lm = fma_rn(t * z, p, t);
     const float ef = (float)e;
-    return __fmaf_rn(ef, 0x1.62e400p-1f, __fmaf_rn(ef, 0x1.7f7d1cp-20f, lm));
+    return fma_rn(ef, 0x1.62e400p-1f, fma_rn(ef, 0x1.7f7d1cp-20f, lm));
 }
 
-__device__ __forceinline__ double log_method(double x) {
-    if (x == 0.0) return -__longlong_as_double(0x7ff0000000000000ll);
-    if (!(x > 0.0) || isinf(x)) return x < 0.0 ? __longlong_as_double(0x7ff8000000000000ll) : x;
-    uint64_t b = (uint64_t)__double_as_longlong(x);
+__host__ __device__ __forceinline__ double log_method(double x) {
+    if (x == 0.0) return -double_of(0x7ff0000000000000ull);
+    if (!(x > 0.0) || std::isinf(x)) return x < 0.0 ? double_of(0x7ff8000000000000ull) : x;
+    uint64_t b = bits_of(x);
     int e = 0;
     if (b < 0x0010000000000000ull) {
-        b = (uint64_t)__double_as_longlong(x * 0x1p54);
+        b = bits_of(x * 0x1p54);
         e = -54;
     }
     e += (int)(b >> 52) - 1023;
@@ -66,23 +121,23 @@ __device__ __forceinline__ double log_method(double x) {
         mb -= 0x0010000000000000ull;
         e += 1;
     }
-    const double m = __longlong_as_double((long long)mb);
+    const double m = double_of(mb);
     const double f = m - 1.0;
     const double s = f / (2.0 + f);
     const double z = s * s;
     const double t = s + s;
-    double p = __fma_rn(z, 0x1.8618618618618p-5, 0x1.af286bca1af28p-5);
-    p = __fma_rn(z, p, 0x1.e1e1e1e1e1e1ep-5);
-    p = __fma_rn(z, p, 0x1.1111111111111p-4);
-    p = __fma_rn(z, p, 0x1.3b13b13b13b14p-4);
-    p = __fma_rn(z, p, 0x1.745d1745d1746p-4);
-    p = __fma_rn(z, p, 0x1.c71c71c71c71cp-4);
-    p = __fma_rn(z, p, 0x1.2492492492492p-3);
-    p = __fma_rn(z, p, 0x1.999999999999ap-3);
-    p = __fma_rn(z, p, 0x1.5555555555555p-2);
-    const double lm = __fma_rn(t * z, p, t);
+    double p = fma_rn(z, 0x1.8618618618618p-5, 0x1.af286bca1af28p-5);
+    p = fma_rn(z, p, 0x1.e1e1e1e1e1e1ep-5);
+    p = fma_rn(z, p, 0x1.1111111111111p-4);
+    p = fma_rn(z, p, 0x1.3b13b13b13b14p-4);
+    p = fma_rn(z, p, 0x1.745d1745d1746p-4);
+    p = fma_rn(z, p, 0x1.c71c71c71c71cp-4);
+    p = fma_rn(z, p, 0x1.2492492492492p-3);
+    p = fma_rn(z, p, 0x1.999999999999ap-3);
+    p = fma_rn(z, p, 0x1.5555555555555p-2);
+    const double lm = fma_rn(t * z, p, t);
     const double ef = (double)e;
-    return __fma_rn(ef, 0x1.62e42fee00000p-1, __fma_rn(ef, 0x1.a39ef35793c76p-33, lm));
+    return fma_rn(ef, 0x1.62e42fee00000p-1, fma_rn(ef, 0x1.a39ef35793c76p-33, lm));
 }
 
 __device__ __forceinline__ void sincos_poly(float r, float &s, float &c) {

@@ -51,6 +51,7 @@
 
 #include "kernel_iface.h"
 #include "octmps_host.h"
+#include "region_consts.h"
 
 using namespace octmps;
 
@@ -227,27 +228,9 @@ octmps_status fill_device(octmps_ctx *ctx, void *dst, int value, size_t bytes) {
 template <typename T>
 void fill_regions(const octmps_sim &s, std::vector<unsigned char> &out) {
     std::vector<RegionConst<T>> r(s.n_regions);
-    for (int i = 0; i < s.n_regions; ++i) {
-        // read_simulation_data (src/octmps_io.cpp:625-626) and
-        // InitDeviceConstantMemory (src/octmps_kernel.cuh:204-214).
-        const double mutr = (s.regions[i].mus == 0.0) ? DBL_MAX
-                                                      : 1.0 / (s.regions[i].mua + s.regions[i].mus);
-        r[i].n = (T)s.regions[i].n;
-        r[i].muas = (T)(1.0 / mutr);
-        r[i].rmuas = (T)mutr;
-        r[i].mua_muas = (T)(s.regions[i].mua * mutr);
-        r[i].g = (T)s.regions[i].g;
-    }
+    fill_region_consts<T>(s, r.data());
     out.resize(sizeof(RegionConst<T>) * r.size());
     memcpy(out.data(), r.data(), out.size());
-}
-
-double div_rd(double a, double b) {
-    double q = a / b;
-    if (!std::isfinite(q) || q == 0.0) return q;
-    double r = std::fma(-q, b, a);
-    if (r != 0.0 && ((r < 0.0) == (b > 0.0))) q = std::nextafter(q, -INFINITY);
-    return q;
 }
 
 octmps_status ensure_planes_d(octmps_ctx *ctx, MeshDev &m) {
