@@ -239,8 +239,9 @@ def run_ours(args, rank, world, local_rank, dist):
         torch.cuda.synchronize()
 
     mid = ctx.upload_mesh(mesh)
-    if args.kernel_form is not None or args.blocks_per_sm:
-        ctx.configure(kernel_form=args.kernel_form or 0, blocks_per_sm=args.blocks_per_sm)
+    if args.kernel_form is not None or args.blocks_per_sm or args.block_size:
+        ctx.configure(kernel_form=args.kernel_form or 0, block_size=args.block_size,
+                      blocks_per_sm=args.blocks_per_sm)
     tuned = None
     if args.autotune:
         tuned = autotune(ctx, mid, sim, xs, roots, args, lanes)
@@ -487,12 +488,14 @@ def reference_step(inp, positions, packets, n_threads):
 
 
 def autotune(ctx, mid, sim, xs, roots, args, lanes):
-    """Launch variant (kernel form, blocks per SM, scatter share) chosen on 4
-    A-scans of the first position."""
+    """Launch variant (kernel form, block size, blocks per SM, scatter share)
+    chosen on 4 A-scans of the first position, at the workload's own lane
+    count (the lane count decides which random numbers a packet draws)."""
     best, table = ctx.autotune(mid, sim, xs[0], roots[0], precision=args.precision,
                                n_photons=args.photons, n_jobs=4, n_lanes=lanes)
-    return {"kernel_form": best[0], "blocks_per_sm": best[1], "scatter_share": best[2],
-            "table_steps_per_s": [[f, b, sh, round(v)] for f, b, sh, v in table]}
+    return {"kernel_form": best[0], "block_size": best[1], "blocks_per_sm": best[2],
+            "scatter_share": best[3],
+            "table_steps_per_s": [[f, bs, b, sh, round(v)] for f, bs, b, sh, _, v in table]}
 
 
 def run_reference(args, rank, world):
@@ -576,6 +579,8 @@ def main():
     ap.add_argument("--kernel-form", type=int, default=None,
                     help="0 per-lane, 1 pooled (default: the library's, or --autotune's)")
     ap.add_argument("--blocks-per-sm", type=int, default=0)
+    ap.add_argument("--block-size", type=int, default=0,
+                    help="threads per block (per-lane 256, 128 or 512; 0 = default)")
     ap.add_argument("--ref-packets", type=int, default=2400,
                     help="packets per A-scan of each --impl reference step")
     args = ap.parse_args()

@@ -189,16 +189,19 @@ octmps_status octmps_ctx_set_multipliers(octmps_ctx *ctx, const uint32_t *a, uin
 
 /* Launch configuration (0 = default).  Two forms of the photon kernel run
  * the same per-photon arithmetic:
- *   per-lane (kernel_form 0, the default): 256-thread blocks, one photon per
- *     thread, a warp vote choosing which half of a propagation step
- *     (boundary test, or scattering) its lanes run;
+ *   per-lane (kernel_form 0, the default): one photon per thread, a warp
+ *     vote choosing which half of a propagation step (boundary test, or
+ *     scattering) its lanes run; blocks of 256 threads (2, 3 or 4 resident
+ *     per SM), 128 (6, 7 or 8) or 512 (2) in the FP32 geometry forms, 256 x 2
+ *     in the FP64 form;
  *   pooled (kernel_form 1): 128-thread blocks; each warp holds two photons
  *     per lane in shared memory and runs every half-step on a full warp of
  *     photons at once (fuller warps, but more instructions and fewer
  *     resident warps: slower on the B-scan workload). */
 typedef struct {
-    int32_t block_size;       /* 0, or the form's block size (256 per-lane, 128 pooled) */
-    int32_t blocks_per_sm;    /* resident blocks per SM: per-lane 2, 3 or 4 (0 = 3; FP64 2);
+    int32_t block_size;       /* per-lane 256 (0 = 256), 128 or 512; pooled 128 (0 = 128) */
+    int32_t blocks_per_sm;    /* resident blocks per SM: per-lane 256 x 2, 3 or 4 (0 = 3),
+                                 128 x 6, 7 or 8 (0 = 6), 512 x 2 (0 = 2); FP64 256 x 2;
                                  pooled 4, 5 or 6 (0 = 4; the FP64 form 2 or 3, 0 = 2) */
     int32_t default_lanes;    /* RNG lanes per job when job.n_lanes = 0 */
     int32_t use_graphs;       /* reserved, 0 (a batch is one persistent launch, so

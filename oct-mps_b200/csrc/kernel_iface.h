@@ -152,21 +152,26 @@ constexpr unsigned int kErrBadNeighbour = 4u; // neighbour index out of range
 
 enum Precision { kMixed = 0, kFP32 = 1, kFP64 = 2 };
 
-// Resident blocks per SM of the default kernel variant, and the share of a
-// warp's live lanes (in 32nds) that must wait for the scattering half of
-// their step before the warp runs it: the best of a sweep on 8 A-scans of the
-// B-scan workload (steps/s, mixed form): 3 blocks (80-register cap) 33.0-33.6 G
-// at shares 10-14, against 28.8-29.3 G with 2 blocks and 28.4-29.1 G with 4.
+// Block size and resident blocks per SM of the default kernel variant, and
+// the share of a warp's live lanes (in 32nds) that must wait for the
+// scattering half of their step before the warp runs it: the best of a sweep
+// on 8 A-scans of the B-scan workload (steps/s, mixed form): 3 blocks
+// (80-register cap) 33.0-33.6 G at shares 10-14, against 28.8-29.3 G with 2
+// blocks and 28.4-29.1 G with 4.
+constexpr int kDefaultBlock = 256;
 constexpr int kDefaultMinBlocks = 3;
 constexpr int kDefaultScatterShare = 12;
 
-// Host-callable launcher (photon_kernel.cu).
-// min_blocks (2, 3 or 4) selects the variant compiled for that many resident
-// blocks per SM; records (test hook) selects the recording variant.
+// Host-callable launcher (photon_kernel.cu).  (block, min_blocks) selects the
+// variant compiled for that block size and that many resident blocks per SM:
+// 256 x 2, 3 or 4; 128 x 6, 7 or 8; 512 x 2 (FP32 geometry forms); the FP64
+// form and the recording variant (records, a test hook) only 256 x 2.
 int launch_photon_kernel(int precision, int min_blocks, const LaunchArgs &args, int grid,
                          int block, void *stream, void *records);
 int photon_kernel_attributes(int precision, int block, int min_blocks, int *regs,
                              int *max_blocks_per_sm);
+// Whether a per-lane variant exists (for configuration checks).
+bool photon_kernel_variant(int precision, int block, int min_blocks);
 
 // Pooled kernel (photon_kernel.cu): 128-thread blocks, each warp holding
 // kPooledPerThread photons per lane in shared memory; min_blocks 4, 5 or 6

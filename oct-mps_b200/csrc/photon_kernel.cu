@@ -29,8 +29,6 @@ namespace octmps {
 
 namespace {
 
-constexpr int kBlock = 256;
-
 // Results of a half-step besides its event code (>= 1): no face reached, the
 // scattering half still to do; or the packet ended on an error.
 constexpr int kEvPending = -1;
@@ -722,16 +720,17 @@ struct Lane {
     uint32_t stall;  // consecutive boundary hits that did not move the photon
 };
 
-// kMinBlocks: resident blocks per SM the register allocation must allow
-// (2: up to 128 registers per thread; 3: up to 80).
-template <typename T, typename P, bool kRecord, int kMinBlocks>
-__global__ void __launch_bounds__(kBlock, kMinBlocks)
+// kBlk threads per block; kMinBlocks: resident blocks per SM the register
+// allocation must allow (65,536 registers per SM: 256 x 3 blocks, up to 80
+// registers per thread; 128 x 7, up to 72; 256 x 2, up to 128).
+template <typename T, typename P, bool kRecord, int kBlk, int kMinBlocks>
+__global__ void __launch_bounds__(kBlk, kMinBlocks)
     photon_kernel(const LaunchArgs args, PacketRecordDev *records) {
     // one split copy per thread (touched only at first biased scatterings and
     // restores, so the record layout's bank conflicts cost little; a table
     // with one column per field measured 10 % slower: its base address is
     // held in registers across the loop)
-    __shared__ SplitCopy<T, P> cont_all[kBlock];
+    __shared__ SplitCopy<T, P> cont_all[kBlk];
     SplitCopy<T, P> &cont = cont_all[threadIdx.x];
     Lane<T, P, kRecord> L;
     L.jd = nullptr;
@@ -766,17 +765,17 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     unsigned long long first_u;
     bool first_ok;
     if (threadIdx.x == 0) {
-        s_busy = kBlock;
+        s_busy = kBlk;
         s_first = 0;
         s_count = 0;
-        if (args.initial_total == 0) s_count = claim_units(args.ctrl, kBlock, s_first);
+        if (args.initial_total == 0) s_count = claim_units(args.ctrl, kBlk, s_first);
     }
     __syncthreads();
     if (args.initial_total == 0) {
         first_u = s_first + threadIdx.x;
         first_ok = threadIdx.x < s_count;
     } else {
-        first_u = args.start_unit + (blockIdx.x * (unsigned long long)kBlock + threadIdx.x);
+        first_u = args.start_unit + (blockIdx.x * (unsigned long long)kBlk + threadIdx.x);
         first_ok = first_u < args.initial_total;
     }
     bool first_unit = true;
@@ -798,7 +797,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
         uint32_t lane;  // its RNG lane (lane counts are 32-bit)
         bool waiting, drain;
     };
-    __shared__ UnitState s_unit[kBlock];
+    __shared__ UnitState s_unit[kBlk];
     UnitState &lg = s_unit[threadIdx.x];
     lg.waiting = lg.drain = false;
     lg.idle_since = lg.last_try = 0;
@@ -1508,22 +1507,35 @@ __global__ void __launch_bounds__(kPoolBlock, kMinBlocks)
 
 namespace {
 
+// Per-lane variants: 256-thread blocks at 2, 3 or 4 per SM, 128-thread
+// blocks at 6, 7 or 8, 512-thread blocks at 2 (FP32 geometry forms); the
+// FP64 form and the recording variant run 256 x 2 (they spill at 80
+// registers).
 template <typename T, typename P>
-const void *pick(int min_blocks, bool record) {
-    if (record) return (const void *)photon_kernel<T, P, true, 2>;
-    switch (min_blocks) {
-        case 2: return (const void *)photon_kernel<T, P, false, 2>;
-        case 3: return (const void *)photon_kernel<T, P, false, 3>;
-        case 4: return (const void *)photon_kernel<T, P, false, 4>;
+const void *pick(int block, int min_blocks, bool record) {
+    if (record) return block == 256 ? (const void *)photon_kernel<T, P, true, 256, 2> : nullptr;
+    if constexpr (sizeof(T) == sizeof(double)) {
+        return block == 256 && min_blocks == 2 ? (const void *)photon_kernel<T, P, false, 256, 2>
+                                               : nullptr;
+    } else {
+    switch (block * 16 + min_blocks) {
+        case 256 * 16 + 2: return (const void *)photon_kernel<T, P, false, 256, 2>;
+        case 256 * 16 + 3: return (const void *)photon_kernel<T, P, false, 256, 3>;
+        case 256 * 16 + 4: return (const void *)photon_kernel<T, P, false, 256, 4>;
+        case 128 * 16 + 6: return (const void *)photon_kernel<T, P, false, 128, 6>;
+        case 128 * 16 + 7: return (const void *)photon_kernel<T, P, false, 128, 7>;
+        case 128 * 16 + 8: return (const void *)photon_kernel<T, P, false, 128, 8>;
+        case 512 * 16 + 2: return (const void *)photon_kernel<T, P, false, 512, 2>;
         default: return nullptr;
+    }
     }
 }
 
-const void *photon_kernel_fn(int precision, int min_blocks, bool record) {
+const void *photon_kernel_fn(int precision, int block, int min_blocks, bool record) {
     switch (precision) {
-        case kMixed: return pick<float, double>(min_blocks, record);
-        case kFP32: return pick<float, float>(min_blocks, record);
-        case kFP64: return pick<double, double>(2, record);  // spills at 80 registers
+        case kMixed: return pick<float, double>(block, min_blocks, record);
+        case kFP32: return pick<float, float>(block, min_blocks, record);
+        case kFP64: return pick<double, double>(block, min_blocks, record);
         default: return nullptr;
     }
 }
@@ -1588,17 +1600,20 @@ int launch_photon_kernel(int precision, int min_blocks, const LaunchArgs &args, 
                          int block, void *stream, void *records) {
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     PacketRecordDev *rec = reinterpret_cast<PacketRecordDev *>(records);
-    if (block != kBlock) return (int)cudaErrorInvalidValue;
-    const void *fn = photon_kernel_fn(precision, min_blocks, rec != nullptr);
+    const void *fn = photon_kernel_fn(precision, block, min_blocks, rec != nullptr);
     if (!fn) return (int)cudaErrorInvalidValue;
     void *params[2] = {const_cast<LaunchArgs *>(&args), &rec};
     return (int)cudaLaunchKernel(fn, dim3(grid), dim3(block), params, 0, st);
 }
 
+bool photon_kernel_variant(int precision, int block, int min_blocks) {
+    return photon_kernel_fn(precision, block, min_blocks, false) != nullptr;
+}
+
 int photon_kernel_attributes(int precision, int block, int min_blocks, int *regs,
                              int *max_blocks_per_sm) {
     cudaFuncAttributes a;
-    const void *fn = photon_kernel_fn(precision, min_blocks, false);
+    const void *fn = photon_kernel_fn(precision, block, min_blocks, false);
     if (!fn) return (int)cudaErrorInvalidValue;
     cudaError_t e = cudaFuncGetAttributes(&a, fn);
     if (e != cudaSuccess) return (int)e;

@@ -314,30 +314,36 @@ octmps_status table_launch(octmps_ctx *ctx, Table &T) {
               : (T.total <= T.total_at_launch || (int)T.running.size() >= kMaxLaunches))
         return OCTMPS_OK;
     // The per-lane kernel (default): 2, 3 or 4 resident 256-thread blocks per
-    // SM (register caps 128, 80, 64); its FP64 form and recording variant
-    // only 2.  The pooled kernel: 4, 5 or 6 resident 128-thread blocks
-    // (caps 128, 96, 80), the FP64 form 2 or 3, the recording variant 2.
+    // SM (register caps 128, 80, 64), 6, 7 or 8 of 128 threads (caps 80, 72,
+    // 64) or 2 of 512 (cap 64); its FP64 form and recording variant only
+    // 256 x 2.  The pooled kernel: 4, 5 or 6 resident 128-thread blocks (caps
+    // 128, 96, 80), the FP64 form 2 or 3, the recording variant 2.
     const bool pooled = ctx->cfg.kernel_form == 1;
     int min_blocks;
+    int lane_block = ctx->cfg.block_size > 0 ? ctx->cfg.block_size : kDefaultBlock;
     if (pooled) {
         const int want = ctx->cfg.blocks_per_sm;
         if (T.prec == kFP64) min_blocks = (want == 2 || want == 3) ? want : kDefaultPooledMinBlocksFP64;
         else min_blocks = (want >= 4 && want <= 6) ? want : kDefaultPooledMinBlocks;
         if (ctx->record_buf) min_blocks = 2;
     } else {
-        min_blocks = ctx->cfg.blocks_per_sm >= 2 && ctx->cfg.blocks_per_sm <= 4
-                         ? ctx->cfg.blocks_per_sm
-                         : kDefaultMinBlocks;
-        if (T.prec == kFP64 || ctx->record_buf) min_blocks = 2;
+        min_blocks = ctx->cfg.blocks_per_sm > 0 ? ctx->cfg.blocks_per_sm
+                     : lane_block == kDefaultBlock ? kDefaultMinBlocks
+                     : lane_block == 128          ? 6
+                                                  : 2;
+        if (T.prec == kFP64 || ctx->record_buf) {
+            lane_block = 256;
+            min_blocks = 2;
+        }
     }
     int regs = 0, per_sm = 0;
     int st = pooled ? pooled_kernel_attributes(T.prec, min_blocks, ctx->record_buf != nullptr, &regs,
                                                &per_sm)
-                    : photon_kernel_attributes(T.prec, 256, min_blocks, &regs, &per_sm);
+                    : photon_kernel_attributes(T.prec, lane_block, min_blocks, &regs, &per_sm);
     if (st) return cuda_fail(ctx, (cudaError_t)st, "kernel attributes");
     if (per_sm < 1) per_sm = 1;
     if (pooled && per_sm > 6) per_sm = 6;  // the split-copy buffers hold 6 blocks per SM
-    const int block = pooled ? kPooledBlock : 256;
+    const int block = pooled ? kPooledBlock : lane_block;
     const uint64_t grid = (uint64_t)ctx->n_sm * per_sm;
     // units the launch's threads take first: one per thread (per-lane), two
     // per thread (pooled)
@@ -395,7 +401,7 @@ octmps_status table_launch(octmps_ctx *ctx, Table &T) {
     CK(cudaEventRecord(L->start, s), "event");
     st = pooled ? launch_pooled_kernel(T.prec, min_blocks, a, (int)grid, s, ctx->record_buf,
                                        T.splits[si])
-                : launch_photon_kernel(T.prec, min_blocks, a, (int)grid, 256, s, ctx->record_buf);
+                : launch_photon_kernel(T.prec, min_blocks, a, (int)grid, block, s, ctx->record_buf);
     if (st) return cuda_fail(ctx, (cudaError_t)st, "photon kernel launch");
     CK(cudaEventRecord(L->stop, s), "event");
     T.total_at_launch = T.total;
@@ -714,13 +720,24 @@ octmps_status octmps_ctx_configure(octmps_ctx *ctx, const octmps_launch_config *
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     if (cfg->kernel_form < 0 || cfg->kernel_form > 1)
         return fail(ctx, OCTMPS_ERR_INVALID_ARG, "kernel_form must be 0 (per-lane) or 1 (pooled)");
-    if (cfg->block_size != 0 && cfg->block_size != (cfg->kernel_form == 0 ? 256 : kPooledBlock))
-        return fail(ctx, OCTMPS_ERR_INVALID_ARG,
-                    "block_size must be 0, 256 (per-lane kernel) or 128 (pooled kernel)");
-    if (cfg->blocks_per_sm != 0 &&
-        (cfg->kernel_form == 0 ? (cfg->blocks_per_sm < 2 || cfg->blocks_per_sm > 4)
-                               : (cfg->blocks_per_sm < 2 || cfg->blocks_per_sm > 6)))
-        return fail(ctx, OCTMPS_ERR_INVALID_ARG, "blocks_per_sm out of range for the kernel form");
+    if (cfg->kernel_form == 1) {
+        if (cfg->block_size != 0 && cfg->block_size != kPooledBlock)
+            return fail(ctx, OCTMPS_ERR_INVALID_ARG, "block_size must be 0 or 128 (pooled kernel)");
+        if (cfg->blocks_per_sm != 0 && (cfg->blocks_per_sm < 2 || cfg->blocks_per_sm > 6))
+            return fail(ctx, OCTMPS_ERR_INVALID_ARG, "blocks_per_sm must be 0 or 2..6 (pooled kernel)");
+    } else {
+        const int b = cfg->block_size > 0 ? cfg->block_size : kDefaultBlock;
+        const int m = cfg->blocks_per_sm > 0 ? cfg->blocks_per_sm
+                      : b == kDefaultBlock ? kDefaultMinBlocks
+                      : b == 128          ? 6
+                                          : 2;
+        // the mixed form's variants (the FP32 form has the same ones; the
+        // FP64 form always runs 256 x 2)
+        if (cfg->block_size < 0 || cfg->blocks_per_sm < 0 || !photon_kernel_variant(kMixed, b, m))
+            return fail(ctx, OCTMPS_ERR_INVALID_ARG,
+                        "per-lane kernel: block_size x blocks_per_sm must be 256 x 2..4, "
+                        "128 x 6..8 or 512 x 2 (0 = default)");
+    }
     if (cfg->scatter_share < 0 || cfg->scatter_share > 32)
         return fail(ctx, OCTMPS_ERR_INVALID_ARG, "scatter_share must be 0..32");
     if (cfg->linger_us < -1 || cfg->linger_us > 1000000)

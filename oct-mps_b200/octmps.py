@@ -359,8 +359,9 @@ class Context:
         self.h = C.c_void_p()
         _check(lib().octmps_ctx_create(device, C.byref(self.h)))
         self._keep = []
-        self._cfg = {"blocks_per_sm": 0, "default_lanes": 0, "hbm_budget_bytes": 0,
-                     "scatter_share": 0, "linger_us": 0, "kernel_form": 0}
+        self._cfg = {"block_size": 0, "blocks_per_sm": 0, "default_lanes": 0,
+                     "hbm_budget_bytes": 0, "scatter_share": 0, "linger_us": 0,
+                     "kernel_form": 0}
         if multipliers is not None:
             self.set_multipliers(multipliers)
 
@@ -383,39 +384,58 @@ class Context:
         _check(lib().octmps_ctx_set_multipliers(self.h, _ptr(a, C.c_uint32), len(a)), self.h)
 
     def configure(self, **settings):
-        """Launch configuration (octmps_launch_config): blocks_per_sm,
-        default_lanes, hbm_budget_bytes, scatter_share, linger_us,
-        kernel_form (0 per-lane, 1 pooled); settings not given keep their
-        current values (0 = default)."""
+        """Launch configuration (octmps_launch_config): block_size,
+        blocks_per_sm, default_lanes, hbm_budget_bytes, scatter_share,
+        linger_us, kernel_form (0 per-lane, 1 pooled); settings not given keep
+        their current values (0 = default)."""
         unknown = set(settings) - set(self._cfg)
         if unknown:
             raise TypeError(f"unknown launch settings: {sorted(unknown)}")
         cfg = dict(self._cfg, **settings)
-        c = LaunchConfig(0, cfg["blocks_per_sm"], cfg["default_lanes"], 0, cfg["hbm_budget_bytes"],
-                         cfg["scatter_share"], cfg["linger_us"], cfg["kernel_form"])
+        c = LaunchConfig(cfg["block_size"], cfg["blocks_per_sm"], cfg["default_lanes"], 0,
+                         cfg["hbm_budget_bytes"], cfg["scatter_share"], cfg["linger_us"],
+                         cfg["kernel_form"])
         _check(lib().octmps_ctx_configure(self.h, C.byref(c)), self.h)
         self._cfg = cfg
+
+    # Default launch variants of autotune(): (kernel_form, block_size,
+    # blocks_per_sm, scatter_share).  Per-lane kernel: 256-thread blocks at
+    # 2-4 per SM and a few scatter shares, 128-thread blocks at 6-8 and
+    # 512-thread blocks at 2 (the register cap follows from block size x
+    # blocks); pooled kernel at 4-5 blocks.
+    AUTOTUNE_VARIANTS = ([(0, 256, 2, 12)] + [(0, 256, 3, sh) for sh in (10, 12, 14)] +
+                         [(0, 256, 4, 12)] + [(0, 128, b, 12) for b in (6, 7, 8)] +
+                         [(0, 512, 2, 12)] + [(1, 128, b, 12) for b in (4, 5)])
 
     def autotune(self, mesh_id, sim, probe_x, root, precision=PREC_MIXED, n_photons=1_000_000,
                  n_jobs=4, n_lanes=0, variants=None, seed=1):
         """Times a sample of the workload (n_jobs jobs of n_photons packets,
         seeds seed..seed+n_jobs-1, in one launch) under each launch variant
-        (kernel form, resident blocks per SM, scatter share) and keeps the
-        fastest, by propagation steps per second of device time.  The sample
-        should keep the whole GPU busy for most of its launch, or the launch's
-        tail decides the ranking.  `variants`: (kernel_form, blocks_per_sm,
-        scatter_share) tuples; by default the per-lane kernel at 2-3 blocks/SM
-        and the pooled kernel at 4-5, each at a few scatter shares.
-        Returns (best, [(kernel_form, blocks_per_sm, scatter_share, steps_per_s), ...])."""
+        and keeps the fastest, by propagation steps per second of device
+        time.  The sample should keep the whole GPU busy for most of its
+        launch, or the launch's tail decides the ranking.
+
+        `variants`: tuples (kernel_form, block_size, blocks_per_sm,
+        scatter_share[, n_lanes]); default AUTOTUNE_VARIANTS.  An n_lanes
+        entry (photons per lane = n_photons / n_lanes) overrides the sample's
+        lane count for that variant: the lane count decides which random
+        numbers each packet draws, so a job's results equal the reference's
+        only at the reference's own lane count, and callers that need that
+        leave it out.  The scatter share is the point at which a warp turns
+        to its waiting scattering halves (the regeneration of its lanes'
+        boundary work), linger_us the point at which idle threads give up.
+        Returns (best, [(kernel_form, block_size, blocks_per_sm, scatter_share,
+        n_lanes, steps_per_s), ...]) and leaves the best variant configured."""
         if variants is None:
-            variants = [(0, b, sh) for b in (2, 3) for sh in (10, 12, 14)] + \
-                       [(1, b, 12) for b in (4, 5)]
+            variants = self.AUTOTUNE_VARIANTS
         nb = sim.num_optical_depth_length_steps
         table = []
-        for form, b, sh in variants:
-            self.configure(kernel_form=form, blocks_per_sm=b, scatter_share=sh)
+        for v in variants:
+            form, block, b, sh = v[:4]
+            lanes = v[4] if len(v) > 4 else n_lanes
+            self.configure(kernel_form=form, block_size=block, blocks_per_sm=b, scatter_share=sh)
             ids = [self.submit(mesh_id, sim, probe_x, root, n_photons=n_photons,
-                               seed=seed + k, n_lanes=n_lanes, precision=precision)
+                               seed=seed + k, n_lanes=lanes, precision=precision)
                    for k in range(n_jobs)]
             self.flush()
             for j in ids:
@@ -425,9 +445,11 @@ class Context:
             for j in ids:
                 self.release(j)
             ms = {s["launch_id"]: s["device_ms"] for s in sts}
-            table.append((form, b, sh, sum(s["steps"] for s in sts) / (sum(ms.values()) / 1e3)))
-        best = max(table, key=lambda r: r[3])
-        self.configure(kernel_form=best[0], blocks_per_sm=best[1], scatter_share=best[2])
+            table.append((form, block, b, sh, lanes,
+                          sum(s["steps"] for s in sts) / (sum(ms.values()) / 1e3)))
+        best = max(table, key=lambda r: r[5])
+        self.configure(kernel_form=best[0], block_size=best[1], blocks_per_sm=best[2],
+                       scatter_share=best[3])
         return best, table
 
     def upload_mesh(self, mesh):

@@ -91,11 +91,11 @@ def test_first_packets_and_tallies_bit_exact(request, ctx, torch_cuda, octmps, o
     """Both kernel forms (0 per-lane, 1 pooled) against the oracle."""
     deck = request.getfixturevalue(deckname)
     lanes, n = 3000, 3000  # one packet per lane
-    ctx.configure(kernel_form=form)
+    ctx.configure(kernel_form=form, block_size=0, blocks_per_sm=0)
     try:
         t_g, st, r_g = run_gpu(ctx, torch_cuda, deck, n, lanes, 985456376, precision)
     finally:
-        ctx.configure(kernel_form=0)
+        ctx.configure(kernel_form=0, block_size=0, blocks_per_sm=0)
     t_o, r_o = run_oracle(oracle, octmps, deck, n, lanes, 985456376, precision, multipliers)
     assert st["packets"] == n
     assert st["steps"] == t_o["steps"] and st["restores"] == t_o["restores"]
@@ -109,11 +109,11 @@ def test_many_packets_per_lane_bit_exact(ctx, torch_cuda, octmps, oracle, multip
                                          precision, form):
     """Lanes run several packets in a row from the same streams (N % lanes != 0)."""
     lanes, n = 997, 20000
-    ctx.configure(kernel_form=form)
+    ctx.configure(kernel_form=form, block_size=0, blocks_per_sm=0)
     try:
         t_g, st, r_g = run_gpu(ctx, torch_cuda, small_deck, n, lanes, 5, precision)
     finally:
-        ctx.configure(kernel_form=0)
+        ctx.configure(kernel_form=0, block_size=0, blocks_per_sm=0)
     t_o, r_o = run_oracle(oracle, octmps, small_deck, n, lanes, 5, precision, multipliers)
     assert st["packets"] == n and st["steps"] == t_o["steps"]
     assert_records_equal(r_g, r_o)
@@ -372,23 +372,39 @@ def test_fp32_forms_keep_the_likelihood_finite(ctx, octmps, layers_deck, precisi
 
 
 def test_autotune_picks_a_variant_and_keeps_results(ctx, octmps, small_deck):
-    """The autotuner times each launch variant (kernel form, blocks per SM,
-    scatter share) on a sample and keeps the fastest; the variants change
-    timing only, never the counts."""
+    """The autotuner times each launch variant (kernel form, block size,
+    blocks per SM, scatter share, optionally lanes) on a sample and keeps the
+    fastest; the launch variants change timing only, never the counts."""
     sim = small_deck["sim"]
     nb = sim.num_optical_depth_length_steps
     mid = ctx.upload_mesh(small_deck["mesh"])
-    variants = [(0, 2, 12), (0, 3, 16), (1, 4, 12), (1, 6, 16)]
+    variants = [(0, 256, 2, 12), (0, 128, 7, 16), (0, 512, 2, 12), (1, 128, 4, 12),
+                (0, 256, 3, 12, 10_000)]
     best, table = ctx.autotune(mid, sim, 0.0, small_deck["root"], n_photons=100_000,
                                n_jobs=2, n_lanes=20_000, variants=variants)
-    assert len(table) == 4 and best in table and all(r[3] > 0 for r in table)
+    assert len(table) == 5 and best in table and all(r[5] > 0 for r in table)
+    assert [r[4] for r in table] == [20_000] * 4 + [10_000]
     runs = []
-    for form, b, sh in ((0, 2, 8), (0, 3, 24), (1, 5, 8), (1, 6, 24)):
-        ctx.configure(kernel_form=form, blocks_per_sm=b, scatter_share=sh)
+    for form, bs, b, sh in ((0, 256, 2, 8), (0, 256, 3, 24), (0, 128, 6, 12), (0, 128, 8, 4),
+                            (0, 512, 2, 20), (1, 128, 5, 8), (1, 128, 6, 24)):
+        ctx.configure(kernel_form=form, block_size=bs, blocks_per_sm=b, scatter_share=sh)
         j = ctx.submit(mid, sim, 0.0, small_deck["root"], n_photons=30_000, seed=3, n_lanes=3000)
         runs.append(ctx.fetch(j, nb))
         ctx.release(j)
-    ctx.configure(kernel_form=0, blocks_per_sm=0, scatter_share=0)
+    ctx.configure(kernel_form=0, block_size=0, blocks_per_sm=0, scatter_share=0)
     for r in runs[1:]:
         assert_tallies_equal(r, runs[0], 0, nb)
     ctx.release_mesh(mid)
+
+
+def test_configure_rejects_launch_variants_that_do_not_exist(ctx, octmps):
+    """Per-lane blocks: 256 x 2..4, 128 x 6..8, 512 x 2; pooled: 128 x 2..6."""
+    for bad in ({"block_size": 128, "blocks_per_sm": 3}, {"block_size": 512, "blocks_per_sm": 3},
+                {"block_size": 64}, {"block_size": 256, "blocks_per_sm": 5},
+                {"kernel_form": 1, "block_size": 256}, {"kernel_form": 1, "blocks_per_sm": 7}):
+        with pytest.raises(octmps.OctmpsError):
+            ctx.configure(**bad)
+    for good in ({"block_size": 128, "blocks_per_sm": 7}, {"block_size": 512},
+                 {"block_size": 128}, {"kernel_form": 1, "blocks_per_sm": 5}):
+        ctx.configure(**good)
+        ctx.configure(kernel_form=0, block_size=0, blocks_per_sm=0)
