@@ -516,26 +516,23 @@ struct Lane {
         int face = -1;
         if (kFused<T>) {
             // FP32 forms: nearest face by perp_i * c_j < perp_j * c_i
-            // (c = -cos > 0), one division for the winner.
-            T best_perp = 0, best_c = 0;
+            // (c = -cos > 0), one division for the winner.  Starting from
+            // (perp, c) = (big, 1) makes the first candidate's test
+            // perp * 1 < big * c, exactly the distance test against big, and
+            // leaves min_d = big / 1 = big when no face is a candidate.
+            T best_perp = DevNum<T>::big, best_c = 1;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                if (cosv[k] < (T)0) {
-                    const T perp = dot3<T>(pl.v[k][0], pl.v[k][1], pl.v[k][2], x, y, z) + pl.v[k][3];
-                    const T c = -cosv[k];
-                    const bool nearer = face < 0 ? perp < DevNum<T>::big * c
-                                                 : perp * best_c < best_perp * c;
-                    if (nearer) {
-                        best_perp = perp;
-                        best_c = c;
-                        face = k;
-                    }
+                const T perp = dot3<T>(pl.v[k][0], pl.v[k][1], pl.v[k][2], x, y, z) + pl.v[k][3];
+                const T c = -cosv[k];
+                if (cosv[k] < (T)0 && perp * best_c < best_perp * c) {
+                    best_perp = perp;
+                    best_c = c;
+                    face = k;
                 }
             }
-            if (face >= 0) {
-                min_d = DevNum<T>::div(best_perp, best_c);
-                min_cos = -best_c;
-            }
+            min_d = DevNum<T>::div(best_perp, best_c);
+            min_cos = -best_c;
         } else {
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
