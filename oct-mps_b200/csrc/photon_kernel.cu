@@ -479,8 +479,8 @@ struct Lane {
     // the general stream's draws keep their order, and the first half of a
     // step no longer diverges on the logarithm.
     __device__ __forceinline__ void draw_step() {
-        const T r = (T)1 - rand_co_G();
-        s_next = -log_method(r) * rg.rmuas;
+        const T r = (T)1 - rand_co_G();  // in [2^-24, 1]: normal
+        s_next = -log_method_normal(r) * rg.rmuas;
     }
 
     // First half of a propagation step, OCTMPSKernel's loop body
@@ -489,21 +489,12 @@ struct Lane {
     // code for finish() (the roulette, called once per step by the loop),
     // kEvPending when no face was reached (the step continues in half_b) or
     // kEvError.
-    template <bool kDrawnAhead = false>
     __device__ __forceinline__ int half_a(unsigned int *err) {
         int ev = 0;
-        // ComputeStepSize, :505-515
-        if (sleft == (T)0) {
-            if (kDrawnAhead) {
-                s = s_next;
-            } else {
-                const T r = (T)1 - rand_co_G();
-                s = -log_method(r) * rg.rmuas;
-            }
-        } else {
-            s = sleft * rg.rmuas;
-            sleft = 0;
-        }
+        // ComputeStepSize, :505-515: a fresh step's size was drawn ahead
+        // (draw_step), a remaining one is converted with the current region's
+        // 1/mu_t
+        s = sleft == (T)0 ? s_next : sleft * rg.rmuas;
         // HitBoundary, :517-572
         Plane4<T> pl;
         pl.load(planes, tet);
@@ -548,10 +539,8 @@ struct Lane {
             }
         }
         const bool hit = s > min_d;
-        if (hit) {
-            sleft = (s - min_d) * rg.muas;
-            s = min_d;
-        }
+        sleft = hit ? (s - min_d) * rg.muas : (T)0;
+        s = hit ? min_d : s;
         stall = (hit && s <= (T)0) ? stall + 1 : 0;
         // Hop, :574-582
         x = DevNum<T>::mad(s, ux, x);
@@ -803,8 +792,14 @@ __global__ void __launch_bounds__(kBlk, kMinBlocks)
     lg.lane = ~0u;
 
     for (;;) {
-        bool has_work = true;
+        // Lanes without a unit (at the start, after a unit's last packet,
+        // while waiting for work) look for one; the warp takes this path
+        // together, so an iteration in which every lane holds a unit costs
+        // one vote for it.
         bool idle = false;
+        unsigned idle_mask = 0u;
+        if (__any_sync(live, packets_left == 0)) {
+        bool has_work = true;
         if (packets_left == 0) {
             unsigned long long u = 0;
             bool got = false;
@@ -876,23 +871,26 @@ __global__ void __launch_bounds__(kBlk, kMinBlocks)
                 }
             }
         }
-        // The two vote sites below are reached by every live lane in every
-        // iteration.
         live = __ballot_sync(live, has_work);
         if (!has_work) break;
-        const unsigned pend = __ballot_sync(live, pending && !idle);
-        const unsigned ready = __ballot_sync(live, !pending && !idle);
+        idle_mask = __ballot_sync(live, idle);
+        if (idle_mask == live) {  // every live lane waits for work
+            __nanosleep(kIdleSleepNs);
+            continue;
+        }
+        }
+        // The vote below is reached by every live lane in every iteration
+        // (an idle lane is never pending).
+        const unsigned pend = __ballot_sync(live, pending);
+        const unsigned ready = live & ~pend & ~idle_mask;
         const bool run_b = ready == 0u || __popc(pend) * 32 >= share * __popc(live);
-        if ((pend | ready) == 0u) __nanosleep(kIdleSleepNs);  // every live lane waits for work
-        if (idle) continue;
+        if (run_b ? !pending : (pending || idle)) continue;
         int ev;
         if (run_b) {
-            if (!pending) continue;
             pending = false;
             ev = L.half_b(cont);
         } else {
-            if (pending) continue;
-            ev = L.template half_a<true>(err);
+            ev = L.half_a(err);
             if (ev == kEvPending) {
                 pending = true;
                 continue;
@@ -907,18 +905,11 @@ __global__ void __launch_bounds__(kBlk, kMinBlocks)
         // move it: a photon on a face moving parallel to it (the cosine of
         // incidence below the grazing limit) is reflected with its direction
         // unchanged, the same hit again at distance 0, forever.
-        unsigned reason = 0;
-        if (!done && steps_packet >= args.step_cap) {
-            atomicOr(err, kErrStepCap);
-            reason = 1;
-        } else if (!done && L.stall >= kStallHits) {
-            reason = 2;
-        }
-        if (reason) {
+        if (!done && (steps_packet >= args.step_cap || L.stall >= kStallHits)) {
+            const unsigned reason = steps_packet >= args.step_cap ? 1u : 2u;
+            if (reason == 1u) atomicOr(err, kErrStepCap);
             atomicAdd(&L.jd->stats[3], 1ull);
             done = true;
-        }
-        if (reason) {
             Incident *inc = args.incident;
             if (inc && atomicCAS(&inc->flag, 0u, reason) == 0u) {
                 inc->slot = (unsigned)lg.slot;
@@ -1400,7 +1391,7 @@ __global__ void __launch_bounds__(kPoolBlock, kMinBlocks)
         int to = 0;  // 0: leaves the pool, 1: stack A, 2: stack B
         if (active) {
             SplitCopy<T, P> &cont = wsplit[m.home];
-            const int ev = run_b ? L.half_b(cont) : L.template half_a<true>(err);
+            const int ev = run_b ? L.half_b(cont) : L.half_a(err);
             const bool step_done = ev != kEvPending;
             const bool end = step_done && (ev == kEvError || L.finish(ev, cont));
             if (!step_done) {

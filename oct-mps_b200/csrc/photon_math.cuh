@@ -106,6 +106,27 @@ __host__ __device__ __forceinline__ float log_method(float x) {
     return fma_rn(ef, 0x1.62e400p-1f, fma_rn(ef, 0x1.7f7d1cp-20f, lm));
 }
 
+// log_method for a positive, finite, normal x (the step-size draws, 1 - a
+// random number in [0, 1): at least 2^-24): the same operations without the
+// special cases, which such an x never reaches.
+__device__ __forceinline__ float log_method_normal(float x) {
+    const uint32_t b = bits_of(x);
+    const bool hi = (b & 0x007fffffu) > 0x003504f3u;  // mantissa above sqrt(2)
+    const uint32_t mb = ((b & 0x007fffffu) | 0x3f800000u) - (hi ? 0x00800000u : 0u);
+    const int e = (int)(b >> 23) - 127 + (hi ? 1 : 0);
+    const float m = float_of(mb);
+    const float f = m - 1.0f;
+    const float s = f / (2.0f + f);
+    const float z = s * s;
+    const float t = s + s;
+    float p = fma_rn(z, 0x1.c71c72p-4f, 0x1.24924ap-3f);
+    p = fma_rn(z, p, 0x1.99999ap-3f);
+    p = fma_rn(z, p, 0x1.555556p-2f);
+    const float lm = fma_rn(t * z, p, t);
+    const float ef = (float)e;
+    return fma_rn(ef, 0x1.62e400p-1f, fma_rn(ef, 0x1.7f7d1cp-20f, lm));
+}
+
 __host__ __device__ __forceinline__ double log_method(double x) {
     if (x == 0.0) return -double_of(0x7ff0000000000000ull);
     if (!(x > 0.0) || std::isinf(x)) return x < 0.0 ? double_of(0x7ff8000000000000ull) : x;
@@ -121,6 +142,31 @@ __host__ __device__ __forceinline__ double log_method(double x) {
         mb -= 0x0010000000000000ull;
         e += 1;
     }
+    const double m = double_of(mb);
+    const double f = m - 1.0;
+    const double s = f / (2.0 + f);
+    const double z = s * s;
+    const double t = s + s;
+    double p = fma_rn(z, 0x1.8618618618618p-5, 0x1.af286bca1af28p-5);
+    p = fma_rn(z, p, 0x1.e1e1e1e1e1e1ep-5);
+    p = fma_rn(z, p, 0x1.1111111111111p-4);
+    p = fma_rn(z, p, 0x1.3b13b13b13b14p-4);
+    p = fma_rn(z, p, 0x1.745d1745d1746p-4);
+    p = fma_rn(z, p, 0x1.c71c71c71c71cp-4);
+    p = fma_rn(z, p, 0x1.2492492492492p-3);
+    p = fma_rn(z, p, 0x1.999999999999ap-3);
+    p = fma_rn(z, p, 0x1.5555555555555p-2);
+    const double lm = fma_rn(t * z, p, t);
+    const double ef = (double)e;
+    return fma_rn(ef, 0x1.62e42fee00000p-1, fma_rn(ef, 0x1.a39ef35793c76p-33, lm));
+}
+
+__device__ __forceinline__ double log_method_normal(double x) {
+    const uint64_t b = bits_of(x);
+    const bool hi = (b & 0x000fffffffffffffull) > 0x0006a09e667f3bcdull;
+    const uint64_t mb =
+        ((b & 0x000fffffffffffffull) | 0x3ff0000000000000ull) - (hi ? 0x0010000000000000ull : 0ull);
+    const int e = (int)(b >> 52) - 1023 + (hi ? 1 : 0);
     const double m = double_of(mb);
     const double f = m - 1.0;
     const double s = f / (2.0 + f);
