@@ -325,7 +325,7 @@ octmps_status octmps_write_result(const char *dir, const octmps_sim *sim, double
  * range; OCTMPS_ERR_KERNEL if the
  * kernel flagged a photon; OCTMPS_ERR_DEVICE on a CUDA error. */
 #define OCTMPS_NOALLOC_MAX_REGIONS 100
-#define OCTMPS_NOALLOC_SCRATCH_BYTES 8240 /* per GPU, held until exit */
+#define OCTMPS_NOALLOC_SCRATCH_BYTES 3440 /* per GPU, held until exit */
 #define OCTMPS_NOALLOC_ROUND16(n) ((((uint64_t)(n)) + 15u) & ~(uint64_t)15u)
 #define OCTMPS_NOALLOC_TALLY_BYTES(nbins) \
     (32u + 2u * OCTMPS_NOALLOC_ROUND16(((uint64_t)(nbins) + 1u) * 8u) + \

@@ -17,17 +17,15 @@ constexpr int kMaxTetsPacked = 1 << kAdjIndexBits;
 
 // Per-region constants as InitDeviceConstantMemory derives them
 // (src/octmps_kernel.cuh:204-214), in the job's geometry precision, followed
-// by the job-invariant subexpressions of the spin arithmetic
-// (region_consts.h derives them): of the region's g, of the job's bias
-// coefficient b and additional bias probability p, and the distance
-// -log(rndStepSizeInTissue) / mu_t.
+// by the two job-invariant terms of the biased spin that cost a square root
+// or a logarithm (region_consts.h derives them): sqrt(1 + b^2) of the job's
+// bias coefficient b, and the distance -log(rndStepSizeInTissue) / mu_t.
+// (Terms that take an add or a multiply are cheaper computed than loaded.)
 template <typename T>
 struct RegionConst {
     T n, muas, rmuas, mua_muas, g;
-    T g_2x, g_1m, g_1m2f, g_1p2, g_1m2;  // g+g, 1-g, mad(-g,g,1), mad(g,g,1), 1-g*g
-    T b_2x, b_1m, b_1p2, b_sq1p2;         // b+b, 1-b, mad(b,b,1), sqrt(mad(b,b,1))
-    T b_c1, b_d1, b_p1, pb_1m;            // sq-1+b, (b+b)(1-b)sq, sq*b*(1-b), 1-p
-    T far;                                // +inf when rndStepSizeInTissue is 0
+    T b_sq1p2;  // sqrt(mad(b, b, 1))
+    T far;      // +inf when rndStepSizeInTissue is 0
 };
 
 // One job (one A-scan) of a launch.  All pointers are device pointers.

@@ -317,18 +317,17 @@ struct Lane {
     }
 
     // SpinTheta, src/octmps_kernel.cuh:807-820, with the current region's g:
-    // temp = (1 - g^2) / (1 + 2 g r - g), cost = (1 + g^2 - temp^2) / 2g, the
-    // terms in g from the region constants.
+    // temp = (1 - g^2) / (1 + 2 g r - g), cost = (1 + g^2 - temp^2) / 2g.
     __device__ __forceinline__ T spin_theta() {
         const RegionConst<T> *c = rc();
         T cost;
-        if (__ldg(&c->g) == (T)0) {
+        const T g = __ldg(&c->g);
+        if (g == (T)0) {
             cost = (T)2 * ((T)1 - rand_co_S()) - (T)1;
         } else {
             const T r = (T)1 - rand_co_S();
-            const T g_2x = __ldg(&c->g_2x);
-            const T temp = DevNum<T>::div(__ldg(&c->g_1m2f), DevNum<T>::mad(g_2x, r, __ldg(&c->g_1m)));
-            cost = DevNum<T>::div(DevNum<T>::mad(-temp, temp, __ldg(&c->g_1p2)), g_2x);
+            const T temp = DevNum<T>::div(DevNum<T>::mad(-g, g, (T)1), DevNum<T>::mad(g + g, r, (T)1 - g));
+            cost = DevNum<T>::div(DevNum<T>::mad(-temp, temp, DevNum<T>::mad(g, g, (T)1)), g + g);
             if (cost < (T)-1) cost = -1;
             else if (cost > (T)1) cost = 1;
         }
@@ -337,18 +336,17 @@ struct Lane {
 
     // SpinThetaForwardFstBias, src/octmps_kernel.cuh:881-896, with the job's
     // bias coefficient b: temp = r / (1 - b) + (1 - r) / sqrt(1 + b^2),
-    // cost = (1 + b^2 - 1 / temp^2) / 2b.
+    // cost = (1 + b^2 - 1 / temp^2) / 2b, the root from the region constants.
     __device__ __forceinline__ T spin_theta_forward() {
         const RegionConst<T> *c = rc();
-        const T b_2x = __ldg(&c->b_2x);
+        const T b = (T)jd->bias_a;
         T cost;
-        if (b_2x == (T)0) {
+        if (b == (T)0) {
             cost = (T)1 - rand_co_S();
         } else {
             const T r = (T)1 - rand_co_S();
-            const T temp = DevNum<T>::div(r, __ldg(&c->b_1m)) +
-                           DevNum<T>::div((T)1 - r, __ldg(&c->b_sq1p2));
-            cost = DevNum<T>::div(__ldg(&c->b_1p2) - DevNum<T>::div((T)1, temp * temp), b_2x);
+            const T temp = DevNum<T>::div(r, (T)1 - b) + DevNum<T>::div((T)1 - r, __ldg(&c->b_sq1p2));
+            cost = DevNum<T>::div(DevNum<T>::mad(b, b, (T)1) - DevNum<T>::div((T)1, temp * temp), b + b);
             if (cost < (T)-1) cost = -1;
             else if (cost > (T)1) cost = 1;
         }
@@ -450,23 +448,25 @@ struct Lane {
             costg1 = fminT(fmaxT(costg1, (T)-1), (T)1);
         }
         if (btmp != (T)0) {
-            // b = btmp (the job's coefficient); the terms in b and g alone
-            // come from the region constants
+            // b = btmp (the job's coefficient); sqrt(1 + b^2) comes from the
+            // region constants
             T f;
             if (reached == 1) {
-                const T b1 = __ldg(&c->b_1p2) - __ldg(&c->b_2x) * cost;
-                const T h1 = __ldg(&c->g_1p2) - __ldg(&c->g_2x) * costg;
-                const T num = __ldg(&c->g_1m2) * __ldg(&c->b_c1) * sqrtT(b1 * b1 * b1);
-                const T den = __ldg(&c->b_d1) * sqrtT(h1 * h1 * h1);
+                const T g = __ldg(&c->g), sq = __ldg(&c->b_sq1p2);
+                const T b1 = DevNum<T>::mad(btmp, btmp, (T)1) - (btmp + btmp) * cost;
+                const T h1 = DevNum<T>::mad(g, g, (T)1) - (g + g) * costg;
+                const T num = ((T)1 - g * g) * (sq - (T)1 + btmp) * sqrtT(b1 * b1 * b1);
+                const T den = (btmp + btmp) * ((T)1 - btmp) * sq * sqrtT(h1 * h1 * h1);
                 f = DevNum<T>::div(num, den);
             } else {
                 const T c1 = sel == 1 ? cost : costg1;
                 const T c2 = sel == 1 ? costg : cost;
-                const T b1 = __ldg(&c->b_1p2) - __ldg(&c->b_2x) * c1;
-                const T pdf1 = DevNum<T>::div(__ldg(&c->b_p1), __ldg(&c->b_c1) * sqrtT(b1 * b1 * b1));
-                const T h2 = sqrtT(__ldg(&c->g_1p2) - __ldg(&c->g_2x) * c2);
-                const T pdf2 = DevNum<T>::div(__ldg(&c->g_1m2), (T)2 * (h2 * h2 * h2));
-                f = DevNum<T>::div(pdf2, DevNum<T>::mad(pb, pdf1, __ldg(&c->pb_1m) * pdf2));
+                const T g = __ldg(&c->g), sq = __ldg(&c->b_sq1p2);
+                const T b1 = DevNum<T>::mad(btmp, btmp, (T)1) - (btmp + btmp) * c1;
+                const T pdf1 = DevNum<T>::div(sq * btmp * ((T)1 - btmp), (sq - (T)1 + btmp) * sqrtT(b1 * b1 * b1));
+                const T h2 = sqrtT(DevNum<T>::mad(g, g, (T)1) - (g + g) * c2);
+                const T pdf2 = DevNum<T>::div((T)1 - g * g, (T)2 * (h2 * h2 * h2));
+                f = DevNum<T>::div(pdf2, DevNum<T>::mad(pb, pdf1, ((T)1 - pb) * pdf2));
             }
             lr *= f;
             if (first) lr_after = lr;

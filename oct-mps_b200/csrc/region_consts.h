@@ -1,16 +1,15 @@
 // Per-region constants of a job, derived on the host (runtime.cu, noalloc.cu).
 //
 // The first five are InitDeviceConstantMemory's (src/octmps_kernel.cuh:204-214)
-// from read_simulation_data's mutr (src/octmps_io.cpp:625-626).  The rest are
-// subexpressions of the spin and likelihood-ratio arithmetic
-// (src/octmps_kernel.cuh:807-820, 881-896, 898-1086) that do not change
-// during a job: g of the region, and the job's bias coefficient a, additional
-// bias probability p and random step size in tissue.  They are evaluated here
-// with the kernel's own operations in the kernel's order (the FP32 forms' fused
-// multiply-adds, the FP64 form's separately rounded products and sums and its
-// round-down division, correctly rounded square root, the project's logarithm),
-// so the kernel reads exactly the values it would otherwise recompute at every
-// scattering.
+// from read_simulation_data's mutr (src/octmps_io.cpp:625-626).  The other two
+// are terms of the biased spin (src/octmps_kernel.cuh:881-896, 898-1086) that
+// do not change during a job and cost a square root or a logarithm: sqrt(1 +
+// b^2) of the bias coefficient b, and -log(rndStepSizeInTissue) / mu_t.  They
+// are evaluated here with the kernel's own operations in the kernel's order
+// (the FP32 forms' fused multiply-adds, the FP64 form's separately rounded
+// products and sums and its round-down division, correctly rounded square
+// root, the project's logarithm), so the kernel reads exactly the values it
+// would otherwise recompute at every scattering.
 #ifndef OCTMPS_REGION_CONSTS_H
 #define OCTMPS_REGION_CONSTS_H
 
@@ -63,21 +62,8 @@ RegionConst<T> region_const(const octmps_region &reg, const octmps_sim &s) {
     c.rmuas = (T)mutr;
     c.mua_muas = (T)(reg.mua * mutr);
     c.g = (T)reg.g;
-    const T g = c.g;
-    c.g_2x = g + g;
-    c.g_1m = (T)1 - g;
-    c.g_1m2f = N::mad(-g, g, (T)1);
-    c.g_1p2 = N::mad(g, g, (T)1);
-    c.g_1m2 = (T)1 - g * g;
     const T b = (T)s.backward_bias_coefficient;
-    c.b_2x = b + b;
-    c.b_1m = (T)1 - b;
-    c.b_1p2 = N::mad(b, b, (T)1);
-    c.b_sq1p2 = std::sqrt(c.b_1p2);
-    c.b_c1 = c.b_sq1p2 - (T)1 + b;
-    c.b_d1 = (b + b) * ((T)1 - b) * c.b_sq1p2;
-    c.b_p1 = c.b_sq1p2 * b * ((T)1 - b);
-    c.pb_1m = (T)1 - (T)s.probability_additional_bias;
+    c.b_sq1p2 = std::sqrt(N::mad(b, b, (T)1));
     const T rs = (T)s.rnd_step_size_in_tissue;
     c.far = rs == (T)0 ? (T)INFINITY : N::div(-log_method(rs), c.muas);
     return c;
