@@ -176,6 +176,20 @@ typedef struct {
                              photon (a packet the reference would run forever) */
 } octmps_job_stats;
 
+/* One detected packet of a job whose sim sets record_photons_flag: the fields
+ * that BiasParam.mco describes for FilteredPhotons.mco ("Weight |
+ * LikelihoodRatio | Radius | AngleRad | OpticalPath | MaxDepth",
+ * src/octmps_io.cpp:259-270; the reference creates the file but writes no
+ * record).  Values in the job's geometry precision, widened exactly. */
+typedef struct {
+    double weight;        /* w (1 - R): the packet weight that leaves through the face */
+    double likelihood;    /* the packet's likelihood ratio */
+    double radius;        /* distance from the probe axis at the exit */
+    double cos_angle;     /* -uz at the exit; the angle to the probe axis is acos of it */
+    double optical_path;
+    double max_depth;
+} octmps_photon_record;
+
 /* ---- context ------------------------------------------------------------ */
 octmps_status octmps_ctx_create(int device, octmps_ctx **out);
 octmps_status octmps_ctx_destroy(octmps_ctx *ctx);
@@ -257,6 +271,17 @@ octmps_status octmps_job_wait(octmps_ctx *ctx, octmps_job_id id, int32_t timeout
 octmps_status octmps_job_fetch(octmps_ctx *ctx, octmps_job_id id, octmps_tally *out);
 octmps_status octmps_job_fetch_stats(octmps_ctx *ctx, octmps_job_id id, octmps_job_stats *out);
 octmps_status octmps_job_release(octmps_ctx *ctx, octmps_job_id id);
+/* RecordPhotonsFlag: records kept per job for jobs whose sim sets
+ * record_photons_flag (0 = the job's packet count, the default); further
+ * detections are counted but not kept.  Applies to jobs submitted after it. */
+octmps_status octmps_ctx_set_photon_record_capacity(octmps_ctx *ctx, uint64_t capacity);
+/* A finished job's detected-packet records, in detection order (which varies
+ * from run to run; the set does not): copies min(kept, max) into `out`
+ * (may be NULL with max 0), sets *n_kept to the records kept and
+ * *n_detected to all detections.  A job without the flag has none. */
+octmps_status octmps_job_photon_records(octmps_ctx *ctx, octmps_job_id id,
+                                        octmps_photon_record *out, uint64_t max,
+                                        uint64_t *n_kept, uint64_t *n_detected);
 
 /* Diagnosis: the first packet of a precision's job table (its current batch,
  * else the latest batch that had one) that was stopped, with the state it
@@ -283,6 +308,12 @@ octmps_status octmps_read_mci(const char *path, octmps_sim *inout);
  * and FilteredPhotons.mco, in directory `dir` ("" = current). */
 octmps_status octmps_write_result(const char *dir, const octmps_sim *sim, double probe_x,
                                   const octmps_tally *t);
+/* Appends detected-packet records to FilteredPhotons.mco in `dir`, one line
+ * per record: the A-scan's probe position, then Weight, LikelihoodRatio,
+ * Radius, AngleRad (acos of cos_angle), OpticalPath, MaxDepth ("%G",
+ * tab-separated). */
+octmps_status octmps_write_filtered_photons(const char *dir, double probe_x,
+                                            const octmps_photon_record *r, uint64_t n);
 
 /* ---- one A-scan without any allocation ----------------------------------------
  * No counterpart in the reference: an addition for callers that cannot

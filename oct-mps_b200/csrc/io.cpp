@@ -190,9 +190,14 @@ extern "C" octmps_status octmps_write_result(const char *dir, const octmps_sim *
                                              const octmps_tally *t) {
     if (!s || !t) return OCTMPS_ERR_INVALID_ARG;
     const int nb = s->num_optical_depth_length_steps;
-    // Write_Bias_Parameters (src/octmps_io.cpp:237-300).
-    FILE *fp = fopen(join(dir, "FilteredPhotons.mco").c_str(), "w");
-    if (fp) fclose(fp);
+    // Write_Bias_Parameters (src/octmps_io.cpp:237-300).  It creates
+    // FilteredPhotons.mco empty; with RecordPhotonsFlag the file holds the
+    // detected-packet records instead (octmps_write_filtered_photons appends
+    // them), so it is left alone here.
+    if (!(short)s->record_photons_flag) {
+        FILE *fp = fopen(join(dir, "FilteredPhotons.mco").c_str(), "w");
+        if (fp) fclose(fp);
+    }
     FILE *b = fopen(join(dir, "BiasParam.mco").c_str(), "w");
     if (!b) return OCTMPS_ERR_IO;
     fprintf(b, "%llu\t\t\t\t\t# Number of filtered photons\n", (unsigned long long)t->num_filtered);
@@ -272,4 +277,18 @@ extern "C" int64_t octmps_safeprimes_read(const char *path, uint32_t *out, uint6
     while (n < max_count && fscanf(f, "%u %u %u", &a, &t1, &t2) == 3) out[n++] = a;
     fclose(f);
     return (int64_t)n;
+}
+
+// FilteredPhotons.mco records (RecordPhotonsFlag): the fields BiasParam.mco
+// lists for the file (src/octmps_io.cpp:259-270), after the A-scan's probe
+// position; the angle is acos of the stored cosine.
+extern "C" octmps_status octmps_write_filtered_photons(const char *dir, double probe_x,
+                                                       const octmps_photon_record *r, uint64_t n) {
+    if (n && !r) return OCTMPS_ERR_INVALID_ARG;
+    FILE *f = fopen(join(dir, "FilteredPhotons.mco").c_str(), "a");
+    if (!f) return OCTMPS_ERR_IO;
+    for (uint64_t i = 0; i < n; ++i)
+        fprintf(f, "%G\t%G\t%G\t%G\t%G\t%G\t%G\n", probe_x, r[i].weight, r[i].likelihood,
+                r[i].radius, acos(r[i].cos_angle), r[i].optical_path, r[i].max_depth);
+    return fclose(f) == 0 ? OCTMPS_OK : OCTMPS_ERR_IO;
 }

@@ -44,7 +44,7 @@ struct alignas(256) JobDesc {
     uint64_t *rng_xS;     // spin stream
     uint32_t *rng_aS;
     void *tally;          // tally block, layout below
-    unsigned long long *stats;  // [0] steps [1] restores [2] packets [3] capped
+    unsigned long long *stats;  // kStatsWords statistics words (below)
     uint64_t n_photons;
     uint32_t n_lanes;
     int32_t n_tets;
@@ -58,7 +58,19 @@ struct alignas(256) JobDesc {
     double shift, bin_width, half_lc;  // OpticalDepthShift, Lc/6, Lc/2 (round-down)
     int32_t root_tet, root_region, type_bias, nbins;
     int32_t n_regions;    // entries of regions[]; a neighbour's region must be below it
+    uint32_t record_cap;  // detected-packet records kept (RecordPhotonsFlag)
+    struct PhotonRecordDev *photon_records;  // null: none kept; index from stats[4]
 };
+
+// One detected packet (RecordPhotonsFlag), laid out as octmps_photon_record.
+struct PhotonRecordDev {
+    double weight, likelihood, radius, cos_angle, optical_path, max_depth;
+};
+
+// Statistics words after a job's tally block: [0] steps [1] restores
+// [2] packets [3] stopped [4] detections recorded (the record index; may pass
+// record_cap), [5..7] unused.
+constexpr int kStatsWords = 8;
 
 static_assert(sizeof(JobDesc) == 256, "a job slot is two cache lines");
 

@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -179,6 +180,15 @@ int main(int argc, char **argv) {
         r.t = octmps_tally{0, 0, 0, r.c1.data(), r.c2.data(), r.s1.data(), r.m1.data(),
                            r.q1.data(), r.s2.data(), r.m2.data(), r.q2.data()};
     }
+    // RecordPhotonsFlag: FilteredPhotons.mco collects the detected-packet
+    // records of every A-scan of the run, written as each A-scan finishes
+    // (lines carry the probe position, so their order does not matter).
+    const bool record = (short)sim.record_photons_flag != 0;
+    std::mutex record_mu;
+    if (record) {
+        FILE *fp = fopen("FilteredPhotons.mco", "w");
+        if (fp) fclose(fp);
+    }
     auto ts = std::chrono::steady_clock::now();
     std::vector<std::thread> threads;
     for (unsigned int g = 0; g < ngpu; ++g) {
@@ -217,6 +227,20 @@ int main(int argc, char **argv) {
                 res[k].st = octmps_job_fetch(ctx, ids[k], &res[k].t);
                 octmps_job_stats js;
                 if (octmps_job_fetch_stats(ctx, ids[k], &js) == OCTMPS_OK) res[k].ms = js.device_ms;
+                uint64_t kept = 0, detected = 0;
+                if (record && res[k].st == OCTMPS_OK &&
+                    octmps_job_photon_records(ctx, ids[k], nullptr, 0, &kept, &detected) == OCTMPS_OK) {
+                    std::vector<octmps_photon_record> recs(kept);
+                    if (octmps_job_photon_records(ctx, ids[k], recs.data(), kept, &kept, &detected) ==
+                        OCTMPS_OK) {
+                        std::lock_guard<std::mutex> lk(record_mu);
+                        octmps_write_filtered_photons("", xs[k], recs.data(), kept);
+                        if (detected > kept)
+                            fprintf(stderr, "A-scan %llu: %llu of %llu detected packets recorded\n",
+                                    (unsigned long long)k, (unsigned long long)kept,
+                                    (unsigned long long)detected);
+                    }
+                }
                 if (res[k].st != OCTMPS_OK)
                     fprintf(stderr, "[GPU %u] failure in OCTMPSKernel: %s\n", g, octmps_last_error(ctx));
                 octmps_job_release(ctx, ids[k]);

@@ -205,10 +205,13 @@ __device__ __forceinline__ void atomic_max_bits<float>(float *addr, float v) {
 // Class I/II tally of one detection, src/octmps_kernel.cuh:684-744.  Out of
 // line (a detection is rare) and given its inputs by value: a member function
 // would take the lane's address and keep the lane's state in local memory
-// instead of registers.  Returns the number of bins the contribution went to.
+// instead of registers.  With RecordPhotonsFlag (a record buffer in the job)
+// it also keeps the packet's record: weight leaving, likelihood ratio, radius
+// rr and cosine -uz at the exit, optical path and maximum depth.  Returns the
+// number of bins the contribution went to.
 template <typename T, typename P>
 __device__ __noinline__ int tally_detection(const JobDesc *jd, P op, T max_depth, T w,
-                                            T r_fresnel, T lr) {
+                                            T r_fresnel, T lr, T rr, T cos_exit) {
     const JobDesc &J = *jd;
     const TallyLayout L = tally_layout(J.nbins, sizeof(P));
     unsigned char *base = reinterpret_cast<unsigned char *>(J.tally);
@@ -221,8 +224,21 @@ __device__ __noinline__ int tally_detection(const JobDesc *jd, P op, T max_depth
     else if (vpf >= (P)4294967295.0) vp = 4294967295ll;
     else vp = (long long)vpf;
     const bool class1 = (P)max_depth > depth - (P)J.half_lc;
-    const T c = w * ((T)1 - r_fresnel) * lr;
+    const T wt = w * ((T)1 - r_fresnel);
+    const T c = wt * lr;
     const P cp = (P)c;
+    if (J.photon_records) {
+        const unsigned long long k = atomicAdd(&J.stats[4], 1ull);
+        if (k < J.record_cap) {
+            PhotonRecordDev &rec = J.photon_records[k];
+            rec.weight = (double)wt;
+            rec.likelihood = (double)lr;
+            rec.radius = (double)rr;
+            rec.cos_angle = (double)cos_exit;
+            rec.optical_path = (double)op;
+            rec.max_depth = (double)max_depth;
+        }
+    }
     // NaN or infinite: counted, and added like any other
     if (!(cp - cp == (P)0)) atomicAdd(&totals[3], 1ull);
     unsigned long long *cnt =
@@ -619,7 +635,8 @@ struct Lane {
                             filt = true;
                     }
                     if (filt) {
-                        const int nbins_added = tally_detection<T, P>(jd, op, max_depth, w, r, lr);
+                        const int nbins_added =
+                            tally_detection<T, P>(jd, op, max_depth, w, r, lr, rr, -uz);
                         if (kRecord) {
                             const P cp = (P)(w * ((T)1 - r) * lr);
                             for (int k = 0; k < nbins_added; ++k) rcontrib += (double)cp;

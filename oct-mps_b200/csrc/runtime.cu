@@ -115,6 +115,8 @@ struct Job {
     void *regions = nullptr;   // RegionConst<T>[n_regions]
     void *tally = nullptr;     // tally block + 4 statistics words
     unsigned long long *stats = nullptr;
+    PhotonRecordDev *records = nullptr;  // RecordPhotonsFlag records, in the tally buffer
+    uint64_t record_cap = 0;
     size_t tally_bytes = 0;
     int slot = -1;             // slot in its table, -1 while waiting for one
     std::shared_ptr<LaunchRec> launch;  // launch that finished its last lane
@@ -166,6 +168,7 @@ struct octmps_ctx {
     octmps_launch_config cfg;
     uint64_t budget = 0;
     uint64_t in_use = 0;
+    uint64_t record_capacity = 0;  // RecordPhotonsFlag records per job (0 = packets)
     std::string err;
     std::recursive_mutex mu;
     void *record_buf = nullptr;  // optional per-lane records of the next launch
@@ -579,6 +582,7 @@ void release_job_device(octmps_ctx *ctx, Job *j) {
     j->regions = nullptr;
     j->tally = nullptr;
     j->stats = nullptr;
+    j->records = nullptr;
     if (ctx->in_use >= j->tally_bytes) ctx->in_use -= j->tally_bytes;
     if (j->rng) {
         if (--j->rng->refs == 0) {
@@ -868,7 +872,15 @@ octmps_status octmps_job_submit(octmps_ctx *ctx, const octmps_job *job, octmps_j
     const size_t psize = job->precision == OCTMPS_PREC_FP32 ? sizeof(float) : sizeof(double);
     const TallyLayout TL = tally_layout(s.num_optical_depth_length_steps, psize);
     const size_t stats_off = TL.bytes;
-    j->tally_bytes = stats_off + 4 * sizeof(unsigned long long);
+    // RecordPhotonsFlag: a record buffer after the statistics words (detections
+    // are at most about one per packet; more are counted, not kept)
+    const uint64_t rec_cap =
+        s.record_photons_flag
+            ? std::min<uint64_t>(ctx->record_capacity ? ctx->record_capacity : n_ph, 0xffffffffull)
+            : 0;
+    const size_t rec_off = stats_off + kStatsWords * sizeof(unsigned long long);
+    j->record_cap = rec_cap;
+    j->tally_bytes = rec_off + rec_cap * sizeof(PhotonRecordDev);
     // RNG lanes: cached per (seed, lanes).
     auto key = std::make_pair(seed, lanes);
     auto ri = ctx->rng_cache.find(key);
@@ -925,9 +937,10 @@ octmps_status octmps_job_submit(octmps_ctx *ctx, const octmps_job *job, octmps_j
                        ctx->stream),
        "regions");
     CK(cudaMallocAsync(&j->tally, j->tally_bytes, ctx->stream), "tally");
-    FILL(j->tally, 0, j->tally_bytes);
+    FILL(j->tally, 0, rec_off);  // tally and statistics; records are written before read
     CK(cudaStreamSynchronize(ctx->stream), "job upload");
     j->stats = reinterpret_cast<unsigned long long *>((char *)j->tally + stats_off);
+    j->records = rec_cap ? reinterpret_cast<PhotonRecordDev *>((char *)j->tally + rec_off) : nullptr;
     ctx->in_use += j->tally_bytes;
     m.refs++;
 
@@ -967,6 +980,8 @@ octmps_status octmps_job_submit(octmps_ctx *ctx, const octmps_job *job, octmps_j
     D.root_tet = job->root_tet;
     D.root_region = m.region[job->root_tet];
     D.n_regions = s.n_regions;
+    D.record_cap = (uint32_t)j->record_cap;
+    D.photon_records = j->records;
     D.type_bias = s.type_bias;
     D.nbins = s.num_optical_depth_length_steps;
 
@@ -1190,6 +1205,39 @@ octmps_status octmps_job_fetch_stats(octmps_ctx *ctx, octmps_job_id id, octmps_j
     }
     out->submit_to_done_ms = j->t_done - j->t_submit;
     return st;
+}
+
+octmps_status octmps_ctx_set_photon_record_capacity(octmps_ctx *ctx, uint64_t capacity) {
+    if (!ctx || capacity > 0xffffffffull) return OCTMPS_ERR_INVALID_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    ctx->record_capacity = capacity;
+    return OCTMPS_OK;
+}
+
+octmps_status octmps_job_photon_records(octmps_ctx *ctx, octmps_job_id id,
+                                        octmps_photon_record *out, uint64_t max,
+                                        uint64_t *n_kept, uint64_t *n_detected) {
+    static_assert(sizeof(octmps_photon_record) == sizeof(PhotonRecordDev),
+                  "record layouts differ");
+    if (!ctx || !n_kept || !n_detected || (max && !out)) return OCTMPS_ERR_INVALID_ARG;
+    octmps_status st = octmps_job_wait(ctx, id, -1);
+    if (st != OCTMPS_OK) return st;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    Job *j = ctx->jobs[id].get();
+    if (!j->stats) return fail(ctx, OCTMPS_ERR_NOT_FOUND, "job already released");
+    unsigned long long s[kStatsWords];
+    CK(cudaMemcpyAsync(s, j->stats, sizeof s, cudaMemcpyDeviceToHost, ctx->stream), "stats");
+    CK(cudaStreamSynchronize(ctx->stream), "stats");
+    *n_detected = j->records ? s[4] : 0;
+    *n_kept = std::min<uint64_t>(*n_detected, j->record_cap);
+    const uint64_t n = std::min<uint64_t>(*n_kept, max);
+    if (n) {
+        CK(cudaMemcpyAsync(out, j->records, n * sizeof(PhotonRecordDev), cudaMemcpyDeviceToHost,
+                           ctx->stream),
+           "records");
+        CK(cudaStreamSynchronize(ctx->stream), "records");
+    }
+    return OCTMPS_OK;
 }
 
 octmps_status octmps_job_release(octmps_ctx *ctx, octmps_job_id id) {

@@ -136,8 +136,15 @@ EXPORTED = [
     "octmps_job_fetch", "octmps_job_fetch_stats", "octmps_job_release", "octmps_read_opt",
     "octmps_read_mci", "octmps_write_result", "octmps_safeprimes_generate",
     "octmps_safeprimes_write", "octmps_safeprimes_read", "octmps_ascan_run_noalloc",
-    "octmps_probe_positions", "octmps_ascans_of_gpu",
+    "octmps_probe_positions", "octmps_ascans_of_gpu", "octmps_ctx_set_photon_record_capacity",
+    "octmps_job_photon_records", "octmps_write_filtered_photons",
 ]
+
+# One detected packet (RecordPhotonsFlag), as octmps_photon_record.
+RECORD_DTYPE = np.dtype([
+    ("weight", np.float64), ("likelihood", np.float64), ("radius", np.float64),
+    ("cos_angle", np.float64), ("optical_path", np.float64), ("max_depth", np.float64),
+])
 
 _lib = None
 
@@ -184,6 +191,11 @@ def lib():
             "octmps_probe_positions": (C.c_int64, [P(Sim), P(C.c_double), C.c_uint64]),
             "octmps_ascans_of_gpu": (C.c_int64, [C.c_uint64, C.c_uint32, C.c_uint32,
                                                  P(C.c_uint64), C.c_uint64]),
+            "octmps_ctx_set_photon_record_capacity": (C.c_int, [C.c_void_p, C.c_uint64]),
+            "octmps_job_photon_records": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p,
+                                                    C.c_uint64, P(C.c_uint64), P(C.c_uint64)]),
+            "octmps_write_filtered_photons": (C.c_int, [C.c_char_p, C.c_double, C.c_void_p,
+                                                        C.c_uint64]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -348,6 +360,13 @@ def tally_struct(t):
 def write_result(directory, sim, probe_x, t):
     _check(lib().octmps_write_result(os.fsencode(directory), C.byref(sim), probe_x,
                                      C.byref(tally_struct(t))))
+
+
+def write_filtered_photons(directory, probe_x, records):
+    """Appends RECORD_DTYPE records to FilteredPhotons.mco in `directory`."""
+    r = np.ascontiguousarray(records, dtype=RECORD_DTYPE)
+    _check(lib().octmps_write_filtered_photons(os.fsencode(directory), probe_x,
+                                               r.ctypes.data if len(r) else None, len(r)))
 
 
 # ---------------------------------------------------------------- context --
@@ -526,6 +545,22 @@ class Context:
 
     def release(self, jid):
         _check(lib().octmps_job_release(self.h, jid), self.h)
+
+    def set_photon_record_capacity(self, capacity):
+        """Records kept per job with RecordPhotonsFlag (0 = the job's packets)."""
+        _check(lib().octmps_ctx_set_photon_record_capacity(self.h, capacity), self.h)
+
+    def photon_records(self, jid):
+        """(records as RECORD_DTYPE in detection order, detections in all) of a
+        finished job whose sim sets record_photons_flag."""
+        kept, det = C.c_uint64(), C.c_uint64()
+        _check(lib().octmps_job_photon_records(self.h, jid, None, 0, C.byref(kept),
+                                               C.byref(det)), self.h)
+        out = np.zeros(kept.value, dtype=RECORD_DTYPE)
+        if kept.value:
+            _check(lib().octmps_job_photon_records(self.h, jid, out.ctypes.data, kept.value,
+                                                   C.byref(kept), C.byref(det)), self.h)
+        return out, det.value
 
     def record_next_launch(self, device_ptr):
         _check(lib().octmps_debug_record_next_launch(self.h, C.c_void_p(device_ptr)), self.h)

@@ -10,11 +10,17 @@
 
 #include <cfloat>
 #include <cmath>
+#include <atomic>
 #include <cstring>
 #include <type_traits>
 #include <vector>
 
 namespace {
+
+// Detected-packet records (oracle_set_photon_records), shared by all threads.
+OraclePhotonRecord *g_records = nullptr;
+uint64_t g_record_cap = 0;
+std::atomic<uint64_t> g_record_n{0};
 
 // ---------------------------------------------------------------- math ---
 
@@ -430,7 +436,7 @@ struct Lane {
     }
 
     // Class I/II tally, src/octmps_kernel.cuh:684-744.
-    void tally_detection(const Photon<T, P> &ph, T r_fresnel) {
+    void tally_detection(const Photon<T, P> &ph, T r_fresnel, T rr) {
         tally.nf++;
         const P op = ph.optical_path;
         const P depth = Num<P>::div(op, (P)2);
@@ -442,8 +448,15 @@ struct Lane {
         else if (vpf >= (P)4294967295.0) vp = 4294967295ll;
         else vp = (int64_t)vpf;
         const bool class1 = (P)ph.max_depth > depth - S.half_lc;
-        const T c = ph.w * ((T)1 - r_fresnel) * ph.lr;
+        const T wt = ph.w * ((T)1 - r_fresnel);
+        const T c = wt * ph.lr;
         const P cp = (P)c;
+        if (g_records) {
+            const uint64_t k = g_record_n.fetch_add(1, std::memory_order_relaxed);
+            if (k < g_record_cap)
+                g_records[k] = {(double)wt, (double)ph.lr, (double)rr, (double)-ph.uz,
+                                (double)op, (double)ph.max_depth};
+        }
         for (int64_t ii = vp - 3; ii < vp + 3; ++ii) {
             if (ii >= 0 && ii < S.nbins) {
                 if (rec) rec_contrib += (double)cp;
@@ -521,7 +534,7 @@ struct Lane {
                         filt = true;
                 }
                 if (filt) {
-                    tally_detection(ph, r);
+                    tally_detection(ph, r, rr);
                     ev |= ORACLE_EV_DETECT;
                 }
             } else {
@@ -1017,6 +1030,12 @@ bool mr_prime(uint64_t n) {
     return true;
 }
 }  // namespace
+
+uint64_t oracle_set_photon_records(OraclePhotonRecord *buf, uint64_t cap) {
+    g_records = buf;
+    g_record_cap = buf ? cap : 0;
+    return g_record_n.exchange(0);
+}
 
 int oracle_safeprimes(uint32_t *out, uint64_t count) {
     const uint64_t chunk = 1 << 16;

@@ -124,6 +124,19 @@ float oracle_uint2float_rz(uint32_t u);
  * safeprimes_base32.txt, src/octmps_kernel.cuh:74-105).  0 on success. */
 int oracle_safeprimes(uint32_t *out, uint64_t count);
 
+/* One detected packet (RecordPhotonsFlag): weight leaving (w (1 - R)),
+ * likelihood ratio, radius and cosine (-uz) at the exit, optical path,
+ * maximum depth; the fields BiasParam.mco lists for FilteredPhotons.mco
+ * (src/octmps_io.cpp:259-270). */
+typedef struct {
+    double weight, likelihood, radius, cos_angle, optical_path, max_depth;
+} OraclePhotonRecord;
+
+/* Runs that follow append their detected-packet records to `buf` (at most
+ * `cap`; buf NULL: none) and count every detection; returns the count since
+ * the last call and resets it. */
+uint64_t oracle_set_photon_records(OraclePhotonRecord *buf, uint64_t cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -63,6 +63,13 @@ class OracleTally(C.Structure):
     ]
 
 
+# One detected packet (RecordPhotonsFlag), as OraclePhotonRecord and the
+# library's octmps_photon_record.
+RECORD_DTYPE = np.dtype([
+    ("weight", np.float64), ("likelihood", np.float64), ("radius", np.float64),
+    ("cos_angle", np.float64), ("optical_path", np.float64), ("max_depth", np.float64),
+])
+
 PACKET_DTYPE = np.dtype([
     ("hash", np.uint64), ("x", np.uint64), ("xR", np.uint64), ("xS", np.uint64),
     ("steps", np.uint32), ("hits", np.uint32), ("scatters", np.uint32),
@@ -169,6 +176,8 @@ class Oracle:
         L.oracle_safeprimes.argtypes = [P(C.c_uint32), C.c_uint64]
         L.oracle_uint2float_rz.restype = C.c_float
         L.oracle_uint2float_rz.argtypes = [C.c_uint32]
+        L.oracle_set_photon_records.restype = C.c_uint64
+        L.oracle_set_photon_records.argtypes = [C.c_void_p, C.c_uint64]
         self.L = L
 
     def safeprimes(self, count):
@@ -211,8 +220,11 @@ class Oracle:
         return out[:min(n, max_steps)]
 
     def run(self, params, mesh, probe, root, n_photons, n_lanes, rng, precision, n_threads=0,
-            record=False):
-        """One A-scan.  mesh: object with region/faces/signs/adj/planes arrays."""
+            record=False, photon_records=0):
+        """One A-scan.  mesh: object with region/faces/signs/adj/planes arrays.
+        record: also return the first packet of every lane.  photon_records: keep
+        up to this many detected-packet records (RECORD_DTYPE, detection order)
+        and return them with the number of detections, (..., records, n)."""
         m = OracleMesh()
         m.n_tets = len(mesh.region)
         m.n_faces = len(mesh.planes)
@@ -224,6 +236,9 @@ class Oracle:
         t = empty_tally(params.nbins)
         ts = _fill_tally_struct(OracleTally, t)
         rec = np.zeros(n_lanes, dtype=PACKET_DTYPE) if record else None
+        precs = np.zeros(photon_records, dtype=RECORD_DTYPE) if photon_records else None
+        self.L.oracle_set_photon_records(precs.ctypes.data if photon_records else None,
+                                         photon_records)
         st = self.L.oracle_run(C.byref(params), C.byref(m), probe[0], probe[1], probe[2], root,
                                n_photons, n_lanes,
                                _ptr(rng["x"], C.c_uint64), _ptr(rng["a"], C.c_uint32),
@@ -231,12 +246,16 @@ class Oracle:
                                _ptr(rng["xS"], C.c_uint64), _ptr(rng["aS"], C.c_uint32),
                                precision, n_threads, C.byref(ts),
                                rec.ctypes.data if record else None)
+        n_det = self.L.oracle_set_photon_records(None, 0)
         if st != 0:
             raise RuntimeError(f"oracle_run failed: {st}")
         for k in ("num_filtered", "num_filtered_class1", "num_filtered_class2", "steps",
                   "restores", "packets", "capped"):
             t[k] = getattr(ts, k)
-        return (t, rec) if record else t
+        out = (t, rec) if record else (t,)
+        if photon_records:
+            out += (precs[:min(n_det, photon_records)], n_det)
+        return out if len(out) > 1 else t
 
 
 class Reference:
