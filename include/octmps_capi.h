@@ -334,7 +334,9 @@ octmps_status octmps_write_filtered_photons(const char *dir, double probe_x,
  * All calls on a device share the array, so calls whose work overlaps on the
  * GPU race: serialise them.  The array's device address is kept per device
  * for the life of the process, so calls after cudaDeviceReset are not
- * supported.  The call returns after the A-scan finished.
+ * supported.  The call returns after the A-scan finished.  It keeps no
+ * detected-packet records (RecordPhotonsFlag is ignored: they would need a
+ * buffer of the caller's; use the job API for them).
  *
  * Device layouts the caller provides:
  *   planes : float, 16 per tet: for face k = 0..3 the reference's face plane
