@@ -6,8 +6,8 @@ leaves, w (1 - R), the likelihood ratio, the radius and cosine at the exit,
 the optical path and the maximum depth.
 
 CPU: the oracle's records against its own tally, and the file writer.  GPU:
-the kernel's records against the oracle's, as sets, bit for bit, in the mixed
-and FP64 forms, and the capacity limit.
+the kernel's records against the oracle's, as sets, bit for bit, in the three
+forms, the capacity limit, and the CLI's file.
 """
 import ctypes as C
 import math
@@ -117,7 +117,7 @@ def gpu_records(ctx, deck, n, lanes, seed, precision):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", [0, 2])
+@pytest.mark.parametrize("precision", [0, 1, 2])
 def test_gpu_records_equal_oracle_records(gpu_ctx, octmps, oracle, multipliers, small_deck,
                                           precision):
     """The kernel's detected-packet records equal the oracle's as a set, bit
