@@ -132,6 +132,23 @@ def test_gpu_records_equal_oracle_records(gpu_ctx, octmps, oracle, multipliers, 
 
 
 @pytest.mark.gpu
+def test_pooled_form_records_equal_oracle_records(gpu_ctx, octmps, oracle, multipliers,
+                                                  small_deck):
+    """The pooled kernel form keeps the same records (it shares the tally)."""
+    gpu_ctx.configure(kernel_form=1, block_size=0, blocks_per_sm=0)
+    try:
+        t_g, r_g, n_g = gpu_records(gpu_ctx, small_deck, 20_000, 2000, 7, 0)
+    finally:
+        gpu_ctx.configure(kernel_form=0, block_size=0, blocks_per_sm=0)
+    _, r_o, n_o = oracle_records(oracle, octmps, small_deck, 20_000, 2000, 7, 0, multipliers,
+                                 100_000)
+    assert n_g == n_o == len(r_g) > 100
+    a, b = sorted_records(r_g), sorted_records(r_o)
+    for f in oracle_py.RECORD_DTYPE.names:
+        np.testing.assert_array_equal(a[f], b[f], err_msg=f)
+
+
+@pytest.mark.gpu
 def test_gpu_record_capacity_and_jobs_without_the_flag(gpu_ctx, octmps, small_deck):
     gpu_ctx.set_photon_record_capacity(10)
     try:
